@@ -1,0 +1,321 @@
+"""Benchmark of the Wilson-flow hot path (FlowSavedGaugeConfigurations).
+
+Workload (the plain FP64 throughput configuration): a 24^3 x 48 lattice
+(shape {48,24,24,24}, x0 = time), generator-G links (seed 7, scale 0.5),
+flowed with eps = 0.01 to t = 3.0 (300 RK3 steps) measuring E and Q at t = 0
+and every 10 steps.  One bench step = one such flow job.  The links
+(382 MB in float64) are larger than the 126 MB L2, so no flush is needed.
+
+metric: site-RK3-steps/s = V * RK3 steps / time (whole job, measurements
+included).  `value`: device time of the flow launches with the links resident
+in HBM (CUDA events on the engine's stream), summed over the K timed jobs,
+max over ranks.  `e2e`: the same jobs through the public C ABI from pinned
+host memory -- upload of the configuration, the flow, and the read-back of
+E(t), Q(t) -- timed on the host around the synchronous calls.
+
+--impl reference runs the LGF reference itself (oracle/_ref/lgf_ref, the
+unmodified sources) on the host cores: one single-rank process per core,
+each flowing an 8^4 sample with the same schedule (10 RK3 steps + one E/Q
+measurement per chunk); value = processes * V * 10 / chunk time.
+
+--gpus N (under torchrun) runs N independent replicas, one per GPU ("replicas
+only": the flow of one lattice does not shard); value sums all ranks' work
+over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SHAPE = (48, 24, 24, 24)
+EPS = 0.01
+NSTEPS = 300
+MEAS = 10
+SEED = 7
+WORKLOAD = "24^3x48 (shape 48,24,24,24) FP64 Wilson flow, eps 0.01 to t=3.0, E/Q at t=0 and every 10 steps"
+# Algorithmic bytes and flops (canonical counts of the scope table):
+#   per site per RK3 step: FP64 4480 B (3 x (read+write 4 links) + su(3)
+#   accumulator), FP32-mixed 2240 B; 42,888 flops.  A stage launch is 1/3.
+BYTES_PER_SITE_STAGE = {0: 4480.0 / 3, 1: 2240.0 / 3}
+FLOPS_PER_SITE_STAGE = 42888.0 / 3
+# DRAM traffic of one stage launch from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum), scaled to this workload; see profiles/.
+NCU_STAGE_TRAFFIC_BYTES = None
+FP64_FMA_PER_SM_PER_CLK = 64  # B200: 64 FP64 FMA lanes per SM (nominal)
+N_SM = 148
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, maxmhz, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                maxmhz = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": maxmhz,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def reduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+# --------------------------------------------------------------- reference
+def run_reference_sample(nproc: int, chunks: int, warm: int):
+    """nproc single-rank reference processes in parallel, each flowing the 8^4
+    config-1 input for `chunks` chunks of 10 RK3 steps + 1 measurement."""
+    from oracle import oracle as O
+    if not O.reference_available():
+        return None, "oracle/_ref/lgf_ref not built"
+    inp = ROOT / "tests" / "golden" / "hb8_seed1.bin"
+
+    def one(_):
+        out = O.run_reference(["cpubench", inp, 8, 8, 8, 8, MEAS * chunks, MEAS], timeout=1800)
+        line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
+        return json.loads(line)
+
+    with ThreadPoolExecutor(max_workers=nproc) as ex:
+        res = list(ex.map(one, range(nproc)))
+    # per chunk: the slowest process defines the aggregate rate
+    per_chunk = [max(r["chunks_s"][c] for r in res) for c in range(warm, chunks)]
+    V = 8 ** 4
+    rates = [nproc * V * MEAS / t for t in per_chunk]
+    return {"value": statistics.median(rates), "per_chunk_s": per_chunk, "cores": nproc,
+            "sample": f"{nproc} parallel single-rank reference processes, 8^4 heatbath config (seed 1), "
+                      f"{chunks} chunks of 10 RK3 steps + 1 E/Q measurement each, first {warm} chunks untimed"}, None
+
+
+def reference_arm(args):
+    world, rank, local, dist = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return
+    nproc = args.ref_procs or os.cpu_count() or 1
+    res, err = run_reference_sample(nproc, args.warmup + args.steps, args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    line = {
+        "impl": "reference",
+        "metric": "site-RK3-steps/s", "value": res["value"], "unit": "site-RK3-steps/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.median(res["per_chunk_s"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "reference_sample": "8^4 per process"},
+        "cpu_baseline": {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"],
+                         "kind": "reference", "sample": res["sample"]},
+        "e2e": {"value": res["value"], "unit": "site-RK3-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ engine
+def engine_arm(args):
+    import numpy as np
+    world, rank, local, dist = dist_setup()
+    from msc_project_b200 import FP32MIXED, FP64, Context
+    from msc_project_b200 import _capi as C
+    prec = FP64 if args.precision == "fp64" else FP32MIXED
+    V = int(np.prod(SHAPE))
+    ctx = Context(local)
+    lat = ctx.lattice(SHAPE, prec)
+    lat.generate(SEED, 0.5)
+    reunit = 10 if prec == FP32MIXED else 0
+    nmeas = 1 + NSTEPS // MEAS
+
+    def job():
+        return lat.flow(EPS, NSTEPS, MEAS, 0.0, True, reunit)
+
+    for _ in range(args.warmup):
+        job()
+    secs = ctypes.c_double()
+    barrier(dist)
+    dev_s = 0.0
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            job()
+            ctx.check(ctx.lib.lgf_last_flow_seconds(lat.h, ctypes.byref(secs)))
+            dev_s += secs.value
+        wall = time.perf_counter() - t0
+    barrier(dist)
+    dev_s = reduce_max(dist, dev_s)
+    value = world * V * NSTEPS * args.steps / dev_s
+
+    # ---- end to end through the public ABI from pinned host memory
+    import torch
+    host = torch.empty(V * 72, dtype=torch.float64, pin_memory=True)
+    links_np = host.numpy()
+    links_np[:] = lat.download()
+    lat2 = ctx.lattice(SHAPE, prec)
+    ptr = ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+    def e2e_job():
+        ctx.check(ctx.lib.lgf_upload_links(lat2.h, ptr))
+        return lat2.flow(EPS, NSTEPS, MEAS, 0.0, True, reunit)
+
+    e2e_job()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_job()
+    e2e_s = reduce_max(dist, time.perf_counter() - t0)
+    e2e_value = world * V * NSTEPS * args.steps / e2e_s
+    lat2.close()
+
+    # ---- dominant kernel: the RK3 stage launch (CUDA events on the engine stream)
+    ms = (ctypes.c_double * 4)()
+    ctx.check(ctx.lib.lgf_profile_kernels(lat.h, EPS, 5, ms))
+    stage_ms = (ms[0] + ms[1] + ms[2]) / 3.0
+    hbm_peak, peak_kind = measured_peaks()
+    stage_bytes = V * BYTES_PER_SITE_STAGE[prec]
+    achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
+    clocks = clk.summary()
+    mhz = clocks["sm_mhz"] or 1965.0
+    fma_peak = N_SM * FP64_FMA_PER_SM_PER_CLK * 2 * mhz * 1e6 / 1e12
+    stage_tflops = V * FLOPS_PER_SITE_STAGE / (stage_ms * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res, err = run_reference_sample(args.ref_procs or os.cpu_count() or 1, 3, 1)
+        if res:
+            cpu = {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"], "kind": "reference",
+                   "sample": res["sample"]}
+        else:
+            cpu = {"value": None, "unavailable": err}
+
+    launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
+    line = {
+        "metric": "site-RK3-steps/s", "value": value, "unit": "site-RK3-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == FP64 else "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": args.precision, "sites": V, "rk3_steps_per_step": NSTEPS,
+                   "measurements_per_step": nmeas, "l2": "inputs larger than L2 (382 MB links)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "site-RK3-steps/s", "h2d_bytes_per_step": V * 72 * 8,
+                "d2h_bytes_per_step": nmeas * 3 * 8},
+        "roofline": {"bound": "hbm", "kernel": "k_rk3_stage (mean of the 3 stages)", "achieved": achieved,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                     "traffic": NCU_STAGE_TRAFFIC_BYTES, "stage_ms": stage_ms, "measure_ms": ms[3]},
+        "fp64_pipe": {"achieved_tflops": stage_tflops, "nominal_peak_tflops_at_clock": fma_peak,
+                      "frac": stage_tflops / fma_peak, "note": "canonical flops / stage time vs 148 SM x 64 FP64 FMA x 2 x median SM clock"},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches_per_job * args.steps,
+        "wall_s": wall,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    lat.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--precision", choices=["fp64", "fp32mixed"], default="fp64")
+    ap.add_argument("--ref-procs", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * lgf_b200.h — C ABI of the B200 Wilson-flow engine (liblgf_b200.so).
+ *
+ * The engine replaces the compute of the LGF reference's
+ * FlowSavedGaugeConfigurations workflow (LGF/LGF.cpp:163-196): the Luscher RK3
+ * gradient flow and the E(t)/Q(t) measurements.  Host code (C++, see
+ * lgf_dropin.h, or any FFI) keeps the reference's parameters, file layout and
+ * outputs and calls these functions with plain pointers and sizes.
+ *
+ * Conventions
+ *   - every function returns an int status: LGF_OK (0) or a negative LGF_E*;
+ *     lgf_last_error(ctx) gives a message for the last failure on that context.
+ *   - host buffers are owned by the caller; device memory is owned by the
+ *     library.  No exceptions and no C++ types cross this boundary.
+ *   - link arrays on the host are float64 in the reference's saved-configuration
+ *     order (LGF/Field/SU3_field.cpp:329-332): for global site
+ *     g = ((x0*N1 + x1)*N2 + x2)*N3 + x3 (x0 slowest, LGF/Lattice/Lattice.cpp:423-436)
+ *     and direction mu = 0..3, the link is 9 complex numbers, row-major,
+ *     (re, im) interleaved, at double offset (g*4 + mu)*18.
+ *   - a context and everything created from it must be used from one host
+ *     thread at a time.  A server (lgf_serve_*) is safe from any threads.
+ */
+#ifndef LGF_B200_H
+#define LGF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LGF_OK 0
+#define LGF_EINVAL (-1)     /* bad argument (shape, precision, null pointer, size) */
+#define LGF_ENOMEM (-2)     /* device allocation failed or admission impossible */
+#define LGF_ECUDA (-3)      /* a CUDA runtime call failed */
+#define LGF_EIO (-4)        /* file could not be read/written */
+#define LGF_ETIMEDOUT (-5)  /* a bounded wait expired */
+#define LGF_ENOTFOUND (-6)  /* unknown job id */
+#define LGF_EBUSY (-7)      /* result not ready yet */
+#define LGF_ESHUTDOWN (-8)  /* server stopped */
+
+#define LGF_PREC_FP64 0       /* the plain form: links and arithmetic in float64 */
+#define LGF_PREC_FP32MIXED 1  /* float32 links/RK3; float64 CH coefficients, reductions */
+
+typedef struct lgf_ctx lgf_ctx;
+typedef struct lgf_lattice lgf_lattice;
+
+int lgf_version(void);
+
+/* One context per GPU.  Replaces mpiWrapper::begin_parallelSession
+ * (LGF/mpiWrapper.cpp:7-16): one process drives one GPU, no halo exchange. */
+int lgf_ctx_create(int device, lgf_ctx** out);
+int lgf_ctx_destroy(lgf_ctx* ctx);
+const char* lgf_last_error(const lgf_ctx* ctx);
+
+/* A device-resident periodic lattice ("torus", LGF/Lattice/Lattice.cpp:447-459).
+ * Every extent must be even (LGF/Lattice/Lattice.cpp:42-49) and >= 4.
+ * Replaces Lattice(params, true) + SU3_field U(lattice, 4) (LGF/LGF.cpp:166,171). */
+int lgf_lattice_create(lgf_ctx* ctx, const int shape[4], int precision, lgf_lattice** out);
+int lgf_lattice_destroy(lgf_lattice* lat);
+/* device bytes a lattice of this shape/precision holds, RK3 scratch included */
+size_t lgf_lattice_footprint(const int shape[4], int precision);
+
+/* Replace SU3_field::loadSU3FromFile / saveSU3ToFile's data movement
+ * (LGF/Field/SU3_field.cpp:260-352, 89-172): V*4*18 doubles, file order. */
+int lgf_upload_links(lgf_lattice* lat, const double* links);
+int lgf_download_links(lgf_lattice* lat, double* links);
+/* Synthetic input: U = exp(i*scale*sum_a h_a lambda_a/2), h_a ~ N(0,1) from a
+ * counter hash of (seed, link, a).  No reference counterpart (input generator). */
+int lgf_generate_links(lgf_lattice* lat, uint64_t seed, double scale);
+
+/* Measurement results, host arrays owned by the caller. */
+typedef struct lgf_meas {
+    int capacity;     /* in: number of slots in t, E, Q (and per-slice arrays) */
+    int count;        /* out: measurements written */
+    double* t;        /* [capacity] flow time of each measurement */
+    double* E;        /* [capacity] energy density, EnergyDensity::calculate */
+    double* Q;        /* [capacity] topological charge, TopologicalCharge::calculate */
+    double* E_slice;  /* [capacity*N0] or NULL: mean e(x) over each x0 slice */
+    double* Q_slice;  /* [capacity*N0] or NULL: each x0 slice's share of Q */
+} lgf_meas;
+
+typedef struct lgf_flow_opts {
+    double eps;          /* flow step epsilon (FlowParameters::getepsilon) */
+    int nsteps;          /* RK3 steps (FlowParameters::getflowSteps) */
+    int meas_every;      /* measure after every k-th step; 0 = never (FlowParameters::getMeasuringInterval) */
+    double t0;           /* flow time at entry (GradientFlow::SetFlowTime, GradientFlow.cpp:64-66) */
+    int measure_at_t0;   /* 1: measure once before the first step (LGF/LGF.cpp:180,184) */
+    int reunit_every;    /* FP32-mixed only: reunitarise every k steps (0 = never) */
+} lgf_flow_opts;
+
+/* The flow loop of FlowSavedGaugeConfigurations (LGF/LGF.cpp:175-188) on the
+ * lattice's current links: GradientFlow::flow (GradientFlow.cpp:22-60) nsteps
+ * times, measuring Q then E (GradientFlow.cpp:77-84) at t0 when asked and after
+ * every meas_every-th step.  t accumulates as t += eps (GradientFlow.cpp:52).
+ * out may be NULL when nothing is measured; otherwise out->capacity must hold
+ * every measurement. */
+int lgf_flow(lgf_lattice* lat, const lgf_flow_opts* opts, lgf_meas* out);
+
+/* One measurement of E and Q now (TopologicalCharge::calculate,
+ * EnergyDensity::calculate).  E_slice/Q_slice may be NULL ([N0] otherwise). */
+int lgf_measure(lgf_lattice* lat, double* E, double* Q, double* E_slice, double* Q_slice);
+/* per-site e(x) = sum_{mu<nu} ReTr(F F) (clover F) and q(x) (improved F,
+ * before the 1/(4 pi^2)), [V] each in global site order; either may be NULL */
+int lgf_site_densities(lgf_lattice* lat, double* e_site, double* q_site);
+/* max over links of ||U^dag U - 1||_F and |det U - 1| */
+int lgf_unitarity(lgf_lattice* lat, double* max_unit_err, double* max_det_err);
+
+/* Diagnostic per-function outputs for parity tests (file-order layouts):
+ *   gradient: Z(x,mu) of Wilson::calculate_FlowGradient (Wilson.cpp:55-71), V*4*18
+ *   fields:   clover F (SU3_field.cpp:533-587) and improved F (:588-597) for
+ *             planes (01,02,03,12,13,23), V*6*18 each (either may be NULL)
+ *   exp:      HermTrLessExp (LGF/Math/SU3_mat.cpp:216-289) of n anti-Hermitian
+ *             traceless matrices, n*18 doubles in and out */
+int lgf_debug_gradient(lgf_lattice* lat, double* Z);
+int lgf_debug_fields(lgf_lattice* lat, double* clover_F, double* improved_F);
+int lgf_exp_su3(lgf_ctx* ctx, int precision, const double* iP, double* out, long long n);
+
+/* Kernel timing for roofline reports (no reference counterpart): launches each
+ * RK3 stage kernel and the measurement kernel nrep times on the lattice's
+ * current links (the links are advanced by the stage launches) and returns
+ * the mean device time per launch in milliseconds, measured with CUDA events
+ * on the engine's stream: ms[0..2] = stages 1..3, ms[3] = measurement. */
+int lgf_profile_kernels(lgf_lattice* lat, double eps, int nrep, double ms[4]);
+/* Device seconds (CUDA events on the engine's stream) of the step and
+ * measurement launches of the last lgf_flow call on this lattice. */
+int lgf_last_flow_seconds(lgf_lattice* lat, double* seconds);
+
+/* ------------------------------------------------------------------ batch */
+/* A flow job: one configuration, its flow schedule and its result arrays. */
+typedef struct lgf_job {
+    int shape[4];
+    int precision;          /* LGF_PREC_* */
+    const double* links;    /* host links in file order, or NULL to generate */
+    uint64_t seed;          /* generator seed when links == NULL */
+    double gen_scale;       /* generator scale when links == NULL (0.5 in the configs) */
+    lgf_flow_opts flow;     /* eps, nsteps, meas_every, t0, measure_at_t0, reunit_every */
+    lgf_meas* meas;         /* results (may be NULL) */
+    double* links_out;      /* optional: final links, file order */
+} lgf_job;
+
+typedef struct lgf_batch_stats {
+    double seconds;         /* device time of the whole batch (CUDA events) */
+    double site_steps;      /* sum over jobs of V * nsteps */
+    int launches;           /* kernel launches (graph nodes) issued */
+    int block_threads;      /* thread-block size chosen for the RK3 stage kernel */
+} lgf_batch_stats;
+
+/* Flow many configurations of uneven volumes together: every RK3 stage of all
+ * jobs is ONE persistent launch over a shared work list of (job, site block)
+ * tiles, each RK3 step of the batch is captured once as a CUDA graph and
+ * replayed, and the stage kernel's block shape is chosen by the autotuner.
+ * Results are identical to flowing each job alone with lgf_flow.  stats may be NULL. */
+int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats);
+
+/* Autotuner: time the candidate block shapes of the RK3 stage kernel for one
+ * precision on a synthetic lattice and remember the fastest for this context
+ * (also used by lgf_batch_run).  best_threads may be NULL. */
+int lgf_autotune(lgf_ctx* ctx, int precision, const int shape[4], int* best_threads);
+
+/* ---------------------------------------------------------------- serving */
+typedef struct lgf_server lgf_server;
+
+typedef struct lgf_serve_config {
+    size_t hbm_budget_bytes;   /* admission budget for resident jobs (links + RK3 scratch) */
+    int max_active;            /* maximum concurrently flowing jobs (slots) */
+    int steps_per_tick;        /* RK3 steps per scheduling tick */
+} lgf_serve_config;
+
+#define LGF_JOB_QUEUED 0
+#define LGF_JOB_RUNNING 1
+#define LGF_JOB_DONE 2
+#define LGF_JOB_FAILED 3
+
+typedef struct lgf_job_status {
+    int state;                 /* LGF_JOB_* */
+    int error;                 /* LGF_* status when FAILED */
+    double submit_s;           /* times on the server's monotonic clock, seconds */
+    double start_s;
+    double end_s;
+    int steps_done;
+} lgf_job_status;
+
+/* A continuous-batching flow server on one context: jobs are admitted by their
+ * HBM footprint as memory and slots free up, flow together in shared launches
+ * with other resident jobs, and leave when done.  The job's arrays (links,
+ * meas, links_out) must stay valid until the job is DONE or FAILED. */
+int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out);
+int lgf_serve_submit(lgf_server* srv, const lgf_job* job, uint64_t* id);
+int lgf_serve_poll(lgf_server* srv, uint64_t id, lgf_job_status* st);
+int lgf_serve_wait(lgf_server* srv, uint64_t id, double timeout_s, lgf_job_status* st);
+int lgf_serve_stop(lgf_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

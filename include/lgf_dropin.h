@@ -1,0 +1,99 @@
+/*
+ * lgf_dropin.h — drop-in replacement for the LGF reference's flow workflows.
+ *
+ * C++ callers keep the reference's parameter classes and entry points:
+ *   SimulationParameters(NrDims, extdofs, shape, beta, cuts, LatticeType)
+ *       (LGF/SimulationParameters.h:3-47)
+ *   FlowParameters(start, stop, flowSteps, epsilon, measureEvery, dataFolder)
+ *       (LGF/SimulationParameters.h:49-86)
+ *   void FlowSavedGaugeConfigurations(SimulationParameters&, FlowParameters&)
+ *       (LGF/LGF.h:31, LGF/LGF.cpp:163-196)
+ *   void ResumeFlowedConfiguration(SimulationParameters&, FlowParameters&, double)
+ *       (LGF/LGF.h:32, LGF/LGF.cpp:197-226)
+ *   void MeasureQdensityDistribution(SimulationParameters&, FlowParameters&)
+ *       (LGF/LGF.h:35, LGF/LGF.cpp:114-124)
+ * with the same input/output files (ensembles/.../*.bin, Observables/.../*.csv)
+ * and the same stdout lines; the flow and the measurements run on the GPU
+ * through lgf_b200.h.  Other languages bind the extern "C" functions at the end.
+ *
+ * Engine selection (no reference counterpart): LGF_PRECISION=fp64|fp32mixed
+ * (default fp64, the plain form) and LGF_DEVICE=<cuda device> in the
+ * environment, or lgf_dropin_configure().
+ */
+#ifndef LGF_DROPIN_H
+#define LGF_DROPIN_H
+
+#ifdef __cplusplus
+#include <string>
+#include <vector>
+
+class SimulationParameters {
+public:
+    /* LatticeType must be "torus" or "torus_OpenT" (LGF/SimulationParameters.h:12-19);
+     * anything else prints the reference's message and exits with EXIT_FAILURE.
+     * The engine flows "torus" only; "torus_OpenT" is rejected at flow time. */
+    SimulationParameters(int NrDims, int extdofs, std::vector<int> shape, double beta, std::vector<int> cuts,
+                         std::string LatticeType = "torus");
+    int getNrDims() { return m_NrDims; }
+    int getextdofs() { return m_extdofs; }
+    int getshape(int i) { return m_shape[i]; }
+    double getbeta() { return m_beta; }
+    int getcuts(int i) { return m_cuts[i]; }
+    std::string getLatticeType() { return m_LatticeType; }
+
+private:
+    int m_NrDims;
+    int m_extdofs;
+    std::vector<int> m_shape;
+    double m_beta;
+    std::vector<int> m_cuts;
+    std::string m_LatticeType;
+};
+
+class FlowParameters {
+public:
+    FlowParameters(int ConfigurationStart, int ConfigurationStop, int flowSteps, double epsilon,
+                   int measure_every_nth_step, const std::string& dataFolder)
+        : m_ConfigurationStart(ConfigurationStart), m_ConfigurationStop(ConfigurationStop), m_flowSteps(flowSteps),
+          m_epsilon(epsilon), m_measure_every_nth_step(measure_every_nth_step), m_dataFolder(dataFolder) {}
+    int getConfigurationStart() { return m_ConfigurationStart; }
+    int getConfigurationStop() { return m_ConfigurationStop; }
+    int getflowSteps() { return m_flowSteps; }
+    double getepsilon() { return m_epsilon; }
+    int getMeasuringInterval() { return m_measure_every_nth_step; }
+    std::string getdataFolder() { return m_dataFolder; }
+
+private:
+    int m_ConfigurationStart;
+    int m_ConfigurationStop;
+    int m_flowSteps;
+    double m_epsilon;
+    int m_measure_every_nth_step;
+    std::string m_dataFolder;
+};
+
+void FlowSavedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams);
+void ResumeFlowedConfiguration(SimulationParameters& params, FlowParameters& flowParams, double flowTime_pickup);
+void MeasureQdensityDistribution(SimulationParameters& params, FlowParameters& flowParams);
+
+extern "C" {
+#endif
+
+/* precision: LGF_PREC_FP64 (0) or LGF_PREC_FP32MIXED (1); reunit_every applies
+ * to the mixed form (0 = never); device = CUDA device ordinal */
+int lgf_dropin_configure(int precision, int reunit_every, int device);
+
+/* Flat C entry points with the reference's arguments (for cgo/ctypes/JNI).
+ * Return 0 on success, a negative LGF_E* status when a configuration failed
+ * (the remaining configurations are still processed). */
+int lgf_dropin_flow_saved(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
+                          double epsilon, int measure_every, const char* data_folder);
+int lgf_dropin_resume_flowed(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
+                             double epsilon, int measure_every, const char* data_folder, double flow_time_pickup);
+int lgf_dropin_measure_qdensity(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
+                                double epsilon, int measure_every, const char* data_folder);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,295 @@
+// Batched flow of many configurations of uneven volumes, and the autotuner.
+//
+// All jobs of one precision are members of one group: every RK3 stage of
+// every job is a single persistent launch over the group's shared tile list,
+// one RK3 step (three stage launches) is captured once as a CUDA graph and
+// replayed, and jobs that finish early leave the work list (the graph reads
+// the list and its length from device memory, so it is not re-captured).
+// Each job's arithmetic is exactly what lgf_flow does for it alone.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "lgf_engine.cuh"
+
+using namespace lgf;
+
+namespace {
+
+struct JobRun {
+    lgf_job* job;
+    LatticeBuf buf;
+    int nmeas = 0;
+    std::vector<double> tvals;
+    double t = 0.0;
+};
+
+int validate_job(lgf_ctx* ctx, const lgf_job& j) {
+    if (!valid_shape(j.shape)) return set_error(ctx, LGF_EINVAL, "job lattice extents must be even and >= 4");
+    if (j.precision != LGF_PREC_FP64 && j.precision != LGF_PREC_FP32MIXED)
+        return set_error(ctx, LGF_EINVAL, "unknown precision %d", j.precision);
+    if (j.flow.nsteps < 0 || j.flow.meas_every < 0 || j.flow.reunit_every < 0)
+        return set_error(ctx, LGF_EINVAL, "negative step count or interval");
+    const int nm = count_measurements(j.flow);
+    if (nm > 0 && (!j.meas || !j.meas->t || !j.meas->E || !j.meas->Q || j.meas->capacity < nm))
+        return set_error(ctx, LGF_EINVAL, "job result arrays missing or capacity < %d", nm);
+    return LGF_OK;
+}
+
+int tune_threads(lgf_ctx* ctx, int prec, const int shape[4], int* best);
+
+int threads_for(lgf_ctx* ctx, int prec, const int shape[4]) {
+    if (ctx->tuned_threads[prec]) return ctx->tuned_threads[prec];
+    int best = default_threads(prec);
+    if (tune_threads(ctx, prec, shape, &best) == LGF_OK) ctx->tuned_threads[prec] = best;
+    return best;
+}
+
+int fetch_results(lgf_ctx* ctx, JobRun& r) {
+    lgf_job& j = *r.job;
+    if (r.nmeas > 0 && j.meas) {
+        const int N0 = r.buf.g.n[0];
+        const size_t per = 2 + 2 * (size_t)N0;
+        std::vector<double> h(per * r.nmeas);
+        LGF_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), r.buf.meas, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        LGF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        for (int m = 0; m < r.nmeas; ++m) {
+            j.meas->t[m] = r.tvals[m];
+            j.meas->E[m] = h[m * per];
+            j.meas->Q[m] = h[m * per + 1];
+            if (j.meas->E_slice) std::memcpy(j.meas->E_slice + (size_t)m * N0, &h[m * per + 2], N0 * sizeof(double));
+            if (j.meas->Q_slice) std::memcpy(j.meas->Q_slice + (size_t)m * N0, &h[m * per + 2 + N0], N0 * sizeof(double));
+        }
+        j.meas->count = r.nmeas;
+    } else if (j.meas) {
+        j.meas->count = 0;
+    }
+    if (j.links_out) return download_links(ctx, r.buf, j.links_out);
+    return LGF_OK;
+}
+
+// Flow one group of jobs (same precision) in lockstep; returns kernel launches.
+int run_group(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, int threads, int* launches) {
+    long long tiles = 0;
+    for (auto* r : runs) tiles += (4LL * r->buf.g.V + threads - 1) / threads;
+    std::unique_ptr<GroupBase> grp(make_group(ctx, prec, threads, (int)runs.size(), std::max(tiles, 1LL), true));
+    if (!grp) return ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
+    std::vector<LatticeBuf*> members;
+    std::vector<double> eps;
+    for (auto* r : runs) {
+        members.push_back(&r->buf);
+        eps.push_back(r->job->flow.eps);
+        r->buf.eps = r->job->flow.eps;
+        LGF_CUDA_TRY(ctx, cudaMemsetAsync(r->buf.slot, 0, sizeof(int), ctx->stream));
+        r->t = r->job->flow.t0;
+    }
+    int rc = grp->set_members(members);
+    if (rc != LGF_OK) return rc;
+    int maxsteps = 0;
+    for (auto* r : runs) maxsteps = std::max(maxsteps, r->job->flow.nsteps);
+
+    std::vector<int> last_measured{-1};
+    auto measure = [&](const std::vector<int>& which) -> int {
+        if (which.empty()) return LGF_OK;
+        if (which != last_measured) {
+            int e = grp->set_measured(which);
+            if (e != LGF_OK) return e;
+            last_measured = which;
+        }
+        *launches += 3;
+        return grp->replay_measure();
+    };
+    // t0 measurements
+    {
+        std::vector<int> which;
+        for (size_t i = 0; i < runs.size(); ++i)
+            if (runs[i]->job->flow.measure_at_t0) {
+                which.push_back((int)i);
+                runs[i]->tvals.push_back(runs[i]->t);
+            }
+        rc = measure(which);
+        if (rc != LGF_OK) return rc;
+    }
+    std::vector<JobRun*> active = runs;
+    for (int s = 1; s <= maxsteps; ++s) {
+        // jobs whose step count is reached leave the work list
+        std::vector<JobRun*> still;
+        for (auto* r : active)
+            if (r->job->flow.nsteps >= s) still.push_back(r);
+        if (still.size() != active.size()) {
+            active = still;
+            members.clear();
+            for (auto* r : active) members.push_back(&r->buf);
+            rc = grp->set_members(members);
+            if (rc != LGF_OK) return rc;
+            last_measured = {-1};
+        }
+        if (active.empty()) break;
+        rc = grp->replay_step();
+        if (rc != LGF_OK) return rc;
+        *launches += grp->launches_per_step();
+        std::vector<int> which;
+        for (size_t i = 0; i < active.size(); ++i) {
+            JobRun* r = active[i];
+            r->t += r->job->flow.eps;  // GradientFlow.cpp:52
+            const lgf_flow_opts& o = r->job->flow;
+            if (prec == LGF_PREC_FP32MIXED && o.reunit_every > 0 && s % o.reunit_every == 0) {
+                rc = launch_reunitarize(ctx, r->buf);
+                if (rc != LGF_OK) return rc;
+                *launches += 1;
+            }
+            if (o.meas_every > 0 && s % o.meas_every == 0) {
+                which.push_back((int)i);
+                r->tvals.push_back(r->t);
+            }
+        }
+        rc = measure(which);
+        if (rc != LGF_OK) return rc;
+    }
+    return LGF_OK;
+}
+
+int tune_threads(lgf_ctx* ctx, int prec, const int shape_in[4], int* best) {
+    // a lattice of the job's shape, capped so tuning stays well under a second
+    int shape[4] = {shape_in[0], shape_in[1], shape_in[2], shape_in[3]};
+    while (1LL * shape[0] * shape[1] * shape[2] * shape[3] > (1LL << 20) && shape[0] > 4) shape[0] = std::max(4, (shape[0] / 2) & ~1);
+    LatticeBuf b;
+    int rc = buf_alloc(ctx, b, shape, prec, 1);
+    if (rc != LGF_OK) return rc;
+    rc = launch_generate(ctx, b, 12345, 0.5);
+    b.eps = 0.01;
+    const int cands[] = {64, 128, 256};
+    float best_ms = 1e30f;
+    int best_t = default_threads(prec);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int th : cands) {
+        if (rc != LGF_OK) break;
+        const long long tiles = (4LL * b.g.V + th - 1) / th;
+        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, th, 1, tiles, false));
+        if (!grp) continue;
+        std::vector<LatticeBuf*> m{&b};
+        if (grp->set_members(m) != LGF_OK) continue;
+        grp->launch_step();  // warm-up
+        cudaEventRecord(e0, ctx->stream);
+        for (int i = 0; i < 3; ++i) grp->launch_step();
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = set_error(ctx, LGF_ECUDA, "autotune timing failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_t = th;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(ctx->stream);
+    buf_free(b);
+    if (rc == LGF_OK) *best = best_t;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lgf_autotune(lgf_ctx* ctx, int precision, const int shape[4], int* best_threads) {
+    if (!ctx) return LGF_EINVAL;
+    if (precision != LGF_PREC_FP64 && precision != LGF_PREC_FP32MIXED) return LGF_EINVAL;
+    if (!valid_shape(shape)) return set_error(ctx, LGF_EINVAL, "autotune shape must be even and >= 4");
+    cudaSetDevice(ctx->device);
+    int best = 0;
+    int rc = tune_threads(ctx, precision, shape, &best);
+    if (rc != LGF_OK) return rc;
+    ctx->tuned_threads[precision] = best;
+    if (best_threads) *best_threads = best;
+    return LGF_OK;
+}
+
+int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats) {
+    if (!ctx || (!jobs && njobs > 0) || njobs < 0) return LGF_EINVAL;
+    cudaSetDevice(ctx->device);
+    for (int i = 0; i < njobs; ++i) {
+        int rc = validate_job(ctx, jobs[i]);
+        if (rc != LGF_OK) return rc;
+    }
+    std::vector<std::unique_ptr<JobRun>> runs;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& r : runs) buf_free(r->buf);
+    };
+    double site_steps = 0.0;
+    for (int i = 0; i < njobs; ++i) {
+        auto r = std::make_unique<JobRun>();
+        r->job = &jobs[i];
+        r->nmeas = count_measurements(jobs[i].flow);
+        int rc = buf_alloc(ctx, r->buf, jobs[i].shape, jobs[i].precision, r->nmeas);
+        if (rc == LGF_OK)
+            rc = jobs[i].links ? upload_links(ctx, r->buf, jobs[i].links)
+                               : launch_generate(ctx, r->buf, jobs[i].seed, jobs[i].gen_scale);
+        runs.push_back(std::move(r));
+        if (rc != LGF_OK) {
+            cleanup();
+            return rc;
+        }
+        site_steps += (double)runs.back()->buf.g.V * jobs[i].flow.nsteps;
+    }
+    // group the jobs by precision and pick each group's block size (autotuned
+    // once per context, before the timed region)
+    std::vector<JobRun*> groups[2];
+    int threads[2] = {0, 0};
+    for (int prec = 0; prec < 2; ++prec) {
+        int big[4] = {4, 4, 4, 4};
+        long long bigV = 0;
+        for (auto& r : runs)
+            if (r->job->precision == prec) {
+                groups[prec].push_back(r.get());
+                if ((long long)r->buf.g.V > bigV) {
+                    bigV = r->buf.g.V;
+                    std::memcpy(big, r->job->shape, sizeof big);
+                }
+            }
+        if (!groups[prec].empty()) threads[prec] = threads_for(ctx, prec, big);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int launches = 0, rc = LGF_OK, threads_used = 0;
+    cudaEventRecord(e0, ctx->stream);
+    for (int prec = 0; prec < 2 && rc == LGF_OK; ++prec) {
+        if (groups[prec].empty()) continue;
+        threads_used = threads[prec];
+        rc = run_group(ctx, prec, groups[prec], threads[prec], &launches);
+    }
+    cudaEventRecord(e1, ctx->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "batch failed: %s", cudaGetErrorString(e));
+    for (auto& r : runs) {
+        if (rc != LGF_OK) break;
+        rc = fetch_results(ctx, *r);
+    }
+    if (stats) {
+        stats->seconds = ms * 1e-3;
+        stats->site_steps = site_steps;
+        stats->launches = launches;
+        stats->block_threads = threads_used;
+    }
+    cleanup();
+    return rc;
+}
+
+}  // extern "C"

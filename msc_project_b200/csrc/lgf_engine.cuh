@@ -1,0 +1,91 @@
+// Internal engine API shared by the C ABI (lgf_capi.cu), the batch runner and
+// the continuous-batching server.  Not installed; no C++ type crosses the
+// public boundary (include/lgf_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lgf_b200.h"
+#include "lgf_kernels.cuh"
+
+struct lgf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    std::string err;
+    int tuned_threads[2] = {0, 0};  // per precision; 0 = not tuned yet
+};
+
+namespace lgf {
+
+int set_error(lgf_ctx* ctx, int code, const char* fmt, ...);
+#define LGF_CUDA_TRY(ctx, call)                                                                          \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return ::lgf::set_error((ctx), LGF_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                    __FILE__, __LINE__);                                                 \
+    } while (0)
+
+bool valid_shape(const int shape[4]);
+size_t footprint_bytes(const int shape[4], int precision, int meas_slots);
+int default_threads(int precision);
+
+// Device resources of one lattice (precision-erased).
+struct LatticeBuf {
+    Geom g{};
+    int prec = LGF_PREC_FP64;
+    void* U[3] = {nullptr, nullptr, nullptr};
+    void* A = nullptr;
+    double2* partial = nullptr;
+    double2* slice_sums = nullptr;
+    double* meas = nullptr;
+    int meas_cap = 0;
+    int* slot = nullptr;
+    int nchunk = 0;
+    double eps = 0.0;
+};
+
+int buf_alloc(lgf_ctx* ctx, LatticeBuf& b, const int shape[4], int precision, int meas_slots);
+int buf_grow_meas(lgf_ctx* ctx, LatticeBuf& b, int meas_slots);
+void buf_free(LatticeBuf& b);
+
+// A set of resident lattices of one precision flowed by shared launches.
+// Launch arguments live in device memory (descriptor table, tile lists and
+// their counts), so a captured CUDA graph stays valid while members change.
+class GroupBase {
+public:
+    virtual ~GroupBase() {}
+    // (re)define the members; order = descriptor index
+    virtual int set_members(const std::vector<LatticeBuf*>& members) = 0;
+    // refresh the eps of the member descriptors (device table)
+    virtual int set_eps(const std::vector<double>& eps) = 0;
+    // the subset of members measured by the next measurement launch
+    virtual int set_measured(const std::vector<int>& which) = 0;
+    virtual int launch_step() = 0;       // one RK3 step of every member (3 stage launches)
+    virtual int launch_measure() = 0;    // measurement of the measured subset (3 launches)
+    virtual int launch_one(int k) = 0;   // one kernel alone: stage k+1 (k<3) or the measurement kernel
+    virtual int capture() = 0;           // capture step and measurement graphs
+    virtual int replay_step() = 0;       // graph launch (captures on first use)
+    virtual int replay_measure() = 0;
+    virtual int launches_per_step() const = 0;
+    virtual int threads() const = 0;
+};
+
+GroupBase* make_group(lgf_ctx* ctx, int precision, int threads, int max_members, long long max_tiles, bool dynamic);
+
+int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b);
+int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file_order);
+int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file_order);
+int launch_generate(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale);
+
+// host->device upload of file-order links through a pinned staging buffer
+int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host);
+int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host);
+
+// measurement schedule of FlowSavedGaugeConfigurations for one job
+int count_measurements(const lgf_flow_opts& o);
+
+}  // namespace lgf

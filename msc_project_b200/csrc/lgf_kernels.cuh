@@ -1,0 +1,593 @@
+// sm_100a kernels of the Wilson-flow engine.
+//
+//   k_rk3_stage<R,S>   one fused Luscher RK3 stage for every link: staple,
+//                      projected force Z, su(3) accumulator update,
+//                      Cayley-Hamilton exponential, link update (ping-pong).
+//                      Replaces Wilson::calculate_FlowGradient
+//                      (LGF/Action/Gauge/Wilson.cpp:55-71), SU3_field::staple
+//                      (LGF/Field/SU3_field.cpp:519-530), HermTrLessExp
+//                      (LGF/Math/SU3_mat.cpp:216-289) and the three update
+//                      loops of GradientFlow::flow (GradientFlow.cpp:22-54).
+//   k_measure<R>       clover F (E) and improved F (q) for every site and plane,
+//                      per-site e(x), q(x), warp-shuffle block partials by
+//                      x0 slice.  Replaces EnergyDensity::calculate and
+//                      TopologicalCharge::calculate (Observables/*.cpp) and the
+//                      loop averages of SU3_field.cpp:533-792.
+//   k_reduce_slices / k_reduce_total
+//                      fixed-order FP64 reductions (per x0 slice, then global)
+//                      in place of MPI_Allreduce; deterministic run to run.
+//   k_to_device / k_to_file    file-order float64 <-> device SoA layout
+//   k_generate_G       synthetic links exp(i s sum_a h_a T^a)
+//   k_reunitarize      FP32-mixed: Gram-Schmidt rows 0,1; row 2 = conj(r0 x r1)
+//   k_unitarity        max ||U^dag U - 1||_F and |det U - 1| per block
+//   k_debug_*          per-function outputs for parity tests
+#pragma once
+#include "lgf_lattice.cuh"
+
+namespace lgf {
+
+// ----------------------------------------------------------------- staple
+// Z = -1/2 [ (W - W^dag) - 1/3 Tr(W - W^dag) ],  W = U_mu(x) A,
+// A = sum_{nu != mu} U_nu(x+mu) (U_nu(x) U_mu(x+nu))^dag
+//                  + (U_mu(x-nu) U_nu(x-nu+mu))^dag U_nu(x-nu)
+template <typename R>
+__device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                                int mu, su3<R>& u_out) {
+    const int V = g.V;
+    su3<R> S;
+    su3_zero(S);
+    const int xpm = fwd(g, s, mu, c.x[mu]);
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        const int xpn = fwd(g, s, nu, c.x[nu]);
+        const int xmn = bwd(g, s, nu, c.x[nu]);
+        const int xmnpm = fwd(g, xmn, mu, c.x[mu]);
+        {
+            su3<R> a2 = load_link(U, V, nu, s);
+            su3<R> a3 = load_link(U, V, mu, xpn);
+            su3<R> t = mul_nn(a2, a3);
+            su3<R> a1 = load_link(U, V, nu, xpm);
+            acc_na(S, a1, t);
+        }
+        {
+            su3<R> b1 = load_link(U, V, mu, xmn);
+            su3<R> b2 = load_link(U, V, nu, xmnpm);
+            su3<R> t = mul_nn(b1, b2);
+            su3<R> b3 = load_link(U, V, nu, xmn);
+            acc_an(S, t, b3);
+        }
+    }
+    u_out = load_link(U, V, mu, s);
+    su3<R> W = mul_nn(u_out, S);
+    return ta_part(W, R(-0.5));
+}
+
+// Device descriptor of one resident lattice.  Every flow launch works on a
+// table of these plus a work list of tiles, so one launch can cover one
+// lattice or many lattices of uneven volumes (batch and serving forms).
+template <typename R> struct LatDesc {
+    Geom g;
+    cplx<R>* U0;          // ring of link buffers: stage 1 U0->U1, 2 U1->U2, 3 U2->U0
+    cplx<R>* U1;
+    cplx<R>* U2;
+    R* A;                 // su(3) RK3 accumulator, 8 coordinates per link
+    double2* partial;     // [N0 * nchunk] block partials of the measurement
+    double2* slice_sums;  // [N0]
+    double* meas;         // [capacity * (2 + 2 N0)] measurement results
+    int* slot;            // next measurement slot
+    int nchunk;           // measurement blocks per x0 slice
+    R eps;
+};
+
+// One RK3 stage (low-storage form of the reference's integrator):
+//   S=1:  A = Z0;                    U1 = exp(eps/4 Z0) U0
+//   S=2:  A = 8/9 Z1 - 17/36 A;      U2 = exp(eps A) U1
+//   S=3:                             U3 = exp(eps (3/4 Z2 - A)) U2
+// which equals GradientFlow.cpp:27-50 term by term.  Input and output are
+// different buffers of the ring (every thread reads neighbours of the input).
+// Persistent: blocks stride over the tile list; tile = (lattice, first link
+// thread); link thread t -> (mu = t / V, s = t % V).
+template <typename R, int S>
+__global__ void __launch_bounds__(256) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
+                                                   const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+        const int2 tile = tiles[ti];
+        const LatDesc<R>* d = descs + tile.x;
+        const Geom g = d->g;
+        const int t = tile.y + threadIdx.x;
+        if (t >= 4 * g.V) continue;
+        const cplx<R>* Uin = S == 1 ? d->U0 : (S == 2 ? d->U1 : d->U2);
+        cplx<R>* Uout = S == 1 ? d->U1 : (S == 2 ? d->U2 : d->U0);
+        R* A = d->A;
+        const R eps = d->eps;
+        const int mu = t / g.V;
+        const int s = t - mu * g.V;
+        const Coord c = site_coord(g, s);
+        su3<R> u;
+        const alg<R> Z = flow_gradient<R>(Uin, g, s, c, mu, u);
+        alg<R> X;
+        if (S == 1) {
+            store_alg(A, g.V, mu, s, Z);
+            X = alg_scale(R(0.25) * eps, Z);
+        } else if (S == 2) {
+            const alg<R> a = load_alg(A, g.V, mu, s);
+            const alg<R> an = alg_axpby(R(8.0 / 9.0), Z, R(-17.0 / 36.0), a);
+            store_alg(A, g.V, mu, s, an);
+            X = alg_scale(eps, an);
+        } else {
+            const alg<R> a = load_alg(A, g.V, mu, s);
+            const alg<R> dd = alg_axpby(R(3.0 / 4.0), Z, R(-1.0), a);
+            X = alg_scale(eps, dd);
+        }
+        const su3<R> E = expm_alg(X);
+        store_link(Uout, g.V, mu, s, mul_nn(E, u));
+    }
+}
+
+// ---------------------------------------------------------- Wilson loops
+// Walks a closed a x b rectangle starting at x in the plane (mu, nu): a step
+// +d multiplies U_d(y) and moves y -> y+d, a step -d moves y -> y-d and
+// multiplies U_d(y)^dag.  Quadrant q selects the leaf, in the orientation the
+// reference uses for all its clover-type averages (SU3_field.cpp:550-560,
+// 606-631, 654-694, 723-775):
+//   q0: +nu^b +mu^a -nu^b -mu^a     q1: +mu^a -nu^b -mu^a +nu^b
+//   q2: -mu^a +nu^b +mu^a -nu^b     q3: -nu^b -mu^a +nu^b +mu^a
+template <typename R> struct Walker {
+    const cplx<R>* __restrict__ U;
+    Geom g;
+    int y, ymu, ynu, mu, nu;
+    su3<R> acc;
+    bool first;
+
+    __device__ __forceinline__ void step(int dir, int sign) {
+        int& yc = (dir == mu) ? ymu : ynu;
+        su3<R> l;
+        if (sign > 0) {
+            l = load_link(U, g.V, dir, y);
+            y = fwd(g, y, dir, yc);
+            yc = wrap_inc(yc, g.n[dir]);
+            if (first) acc = l;
+            else acc = mul_nn(acc, l);
+        } else {
+            y = bwd(g, y, dir, yc);
+            yc = wrap_dec(yc, g.n[dir]);
+            l = load_link(U, g.V, dir, y);
+            if (first) {
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc)
+                        acc.m[3 * r + cc] = cmk<R>(l.m[3 * cc + r].re, -l.m[3 * cc + r].im);
+            } else {
+                acc = mul_na(acc, l);
+            }
+        }
+        first = false;
+    }
+    __device__ __forceinline__ void seg(int dir, int sign, int len) {
+        for (int i = 0; i < len; ++i) step(dir, sign);
+    }
+};
+
+template <typename R, int A, int B>
+__device__ __forceinline__ void add_leaves(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c, int mu,
+                                           int nu, su3<R>& sum) {
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        Walker<R> w;
+        w.U = U;
+        w.g = g;
+        w.y = s;
+        w.ymu = c.x[mu];
+        w.ynu = c.x[nu];
+        w.mu = mu;
+        w.nu = nu;
+        w.first = true;
+        if (q == 0) { w.seg(nu, +1, B); w.seg(mu, +1, A); w.seg(nu, -1, B); w.seg(mu, -1, A); }
+        else if (q == 1) { w.seg(mu, +1, A); w.seg(nu, -1, B); w.seg(mu, -1, A); w.seg(nu, +1, B); }
+        else if (q == 2) { w.seg(mu, -1, A); w.seg(nu, +1, B); w.seg(mu, +1, A); w.seg(nu, -1, B); }
+        else { w.seg(nu, -1, B); w.seg(mu, -1, A); w.seg(nu, +1, B); w.seg(mu, +1, A); }
+        su3_addto(sum, w.acc);
+    }
+}
+
+// Clover F and improved F for plane (mu, nu) at site s:
+//   F   = F[C11],  C11 = 1/4 (1x1 leaves)
+//   F^  = 19/9 F[C11] + 1/36 F[C22] - 32/45 F[C12] + 1/15 F[C13]
+// with C22 = 1/4 (2x2), C12 = 1/8 (1x2 + 2x1), C13 = 1/8 (1x3 + 3x1)
+// (SU3_field.cpp:588-597).
+template <typename R>
+__device__ __forceinline__ void plane_fields(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                             int mu, int nu, alg<R>& F11, alg<R>& Fhat) {
+    su3<R> C;
+    su3_zero(C);
+    add_leaves<R, 1, 1>(U, g, s, c, mu, nu, C);
+    F11 = field_strength(C, R(0.25));
+    Fhat = alg_scale(R(19.0 / 9.0), F11);
+    su3_zero(C);
+    add_leaves<R, 2, 2>(U, g, s, c, mu, nu, C);
+    alg<R> f = field_strength(C, R(0.25));
+    Fhat = alg_axpby(R(1), Fhat, R(1.0 / 36.0), f);
+    su3_zero(C);
+    add_leaves<R, 1, 2>(U, g, s, c, mu, nu, C);
+    add_leaves<R, 2, 1>(U, g, s, c, mu, nu, C);
+    f = field_strength(C, R(1.0 / 8.0));
+    Fhat = alg_axpby(R(1), Fhat, R(-32.0 / 45.0), f);
+    su3_zero(C);
+    add_leaves<R, 1, 3>(U, g, s, c, mu, nu, C);
+    add_leaves<R, 3, 1>(U, g, s, c, mu, nu, C);
+    f = field_strength(C, R(1.0 / 8.0));
+    Fhat = alg_axpby(R(1), Fhat, R(1.0 / 15.0), f);
+}
+
+__device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
+__device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
+
+constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
+
+// Measurement tile = (lattice, x0 slice, chunk of 32 consecutive sites of the
+// slice); 6 warps = 6 planes.  Writes the tile's sums of e(x) and q(x) to the
+// lattice's partial[slice * nchunk + chunk] (double2) and, when site_e/site_q
+// are not null (single-lattice use), e(x) and q(x) per site.
+//   e(x) = sum_{mu<nu} ReTr(F F)                 (EnergyDensity.cpp:13-20)
+//   q(x) = ReTr(F^32 F^01) + ReTr(F^31 F^20) + ReTr(F^30 F^12)
+//        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
+//                                             (TopologicalCharge.cpp:11-16)
+template <typename R>
+__global__ void __launch_bounds__(MEAS_SITES * 6) k_measure(const LatDesc<R>* __restrict__ descs,
+                                                            const int4* __restrict__ mtiles,
+                                                            const int* __restrict__ nmtiles,
+                                                            double* __restrict__ site_e, double* __restrict__ site_q) {
+    __shared__ alg<R> sF[6][MEAS_SITES];
+    __shared__ double sE[6][MEAS_SITES];
+    const int lane = threadIdx.x, p = threadIdx.y;
+    const int n = *nmtiles;
+    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+        const int4 tile = mtiles[ti];
+        const LatDesc<R>* d = descs + tile.x;
+        const Geom g = d->g;
+        const int slice = tile.y, chunk = tile.z;
+        const int off = chunk * MEAS_SITES + lane;
+        const bool valid = off < g.Vs;
+        const int s = slice * g.Vs + (valid ? off : 0);
+        if (valid) {
+            const Coord c = site_coord(g, s);
+            alg<R> F11, Fh;
+            plane_fields<R>(d->U0, g, s, c, c_plane_mu[p], c_plane_nu[p], F11, Fh);
+            sF[p][lane] = Fh;
+            sE[p][lane] = retr_hh(F11, F11);
+        }
+        __syncthreads();
+        if (p == 0) {
+            double e = 0.0, q = 0.0;
+            if (valid) {
+                e = ((sE[0][lane] + sE[1][lane]) + (sE[2][lane] + sE[3][lane])) + (sE[4][lane] + sE[5][lane]);
+                q = -retr_hh(sF[5][lane], sF[0][lane]) + retr_hh(sF[4][lane], sF[1][lane]) -
+                    retr_hh(sF[2][lane], sF[3][lane]);
+                if (site_e) site_e[s] = e;
+                if (site_q) site_q[s] = q;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                e += __shfl_xor_sync(0xffffffffu, e, o);
+                q += __shfl_xor_sync(0xffffffffu, q, o);
+            }
+            if (lane == 0) d->partial[slice * d->nchunk + chunk] = make_double2(e, q);
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int RED_THREADS = 256;
+
+// Slice sums in fixed order (deterministic run to run): thread i sums chunks
+// i, i+256, ... sequentially, then a fixed binary tree.  One block per
+// (lattice, slice) entry of rtiles.  Result slot layout per measurement:
+// [E, Q, E_slice[N0], Q_slice[N0]] at meas + (*slot) * (2 + 2 N0).
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_slices(const LatDesc<R>* __restrict__ descs,
+                                                               const int2* __restrict__ rtiles,
+                                                               const int* __restrict__ nrtiles) {
+    __shared__ double se[RED_THREADS], sq[RED_THREADS];
+    const int n = *nrtiles;
+    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+        const int2 tile = rtiles[ti];
+        const LatDesc<R>* d = descs + tile.x;
+        const int t = tile.y;
+        const int nchunk = d->nchunk;
+        double e = 0.0, q = 0.0;
+        for (int j = threadIdx.x; j < nchunk; j += RED_THREADS) {
+            const double2 v = d->partial[t * nchunk + j];
+            e += v.x;
+            q += v.y;
+        }
+        se[threadIdx.x] = e;
+        sq[threadIdx.x] = q;
+        __syncthreads();
+        for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) {
+                se[threadIdx.x] += se[threadIdx.x + w];
+                sq[threadIdx.x] += sq[threadIdx.x + w];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const int N0 = d->g.n[0];
+            const double inv4pi2 = 1.0 / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+            double* o = d->meas + (size_t)(*d->slot) * (2 + 2 * N0);
+            o[2 + t] = se[0] / (double)d->g.Vs;
+            o[2 + N0 + t] = sq[0] * inv4pi2;
+            d->slice_sums[t] = make_double2(se[0], sq[0]);
+        }
+        __syncthreads();
+    }
+}
+
+// Global sums over the slices (fixed tree), one block per lattice in jobs[].
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_total(const LatDesc<R>* __restrict__ descs,
+                                                              const int* __restrict__ jobs,
+                                                              const int* __restrict__ njobs) {
+    __shared__ double se[RED_THREADS], sq[RED_THREADS];
+    const int n = *njobs;
+    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+        const LatDesc<R>* d = descs + jobs[ti];
+        const int N0 = d->g.n[0];
+        double e = 0.0, q = 0.0;
+        for (int j = threadIdx.x; j < N0; j += RED_THREADS) {
+            e += d->slice_sums[j].x;
+            q += d->slice_sums[j].y;
+        }
+        se[threadIdx.x] = e;
+        sq[threadIdx.x] = q;
+        __syncthreads();
+        for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) {
+                se[threadIdx.x] += se[threadIdx.x + w];
+                sq[threadIdx.x] += sq[threadIdx.x + w];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const double inv4pi2 = 1.0 / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+            double* o = d->meas + (size_t)(*d->slot) * (2 + 2 * N0);
+            o[0] = se[0] * (1.0 / (double)d->g.V);  // EnergyDensity.cpp:26
+            o[1] = sq[0] * inv4pi2;                 // TopologicalCharge.cpp:21
+            *d->slot = *d->slot + 1;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------- layouts
+// file order (double, [s][mu][k][re,im]) -> device SoA in precision R
+template <typename R>
+__global__ void k_to_device(const double2* __restrict__ file, cplx<R>* __restrict__ U, int V) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * V) return;
+    const int mu = t / V, s = t - mu * V;
+    const double2* src = file + ((size_t)s * 4 + mu) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const double2 v = src[k];
+        U[((size_t)mu * 9 + k) * V + s] = cmk<R>((R)v.x, (R)v.y);
+    }
+}
+template <typename R>
+__global__ void k_to_file(const cplx<R>* __restrict__ U, double2* __restrict__ file, int V) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * V) return;
+    const int mu = t / V, s = t - mu * V;
+    double2* dst = file + ((size_t)s * 4 + mu) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const cplx<R> z = U[((size_t)mu * 9 + k) * V + s];
+        dst[k] = make_double2((double)z.re, (double)z.im);
+    }
+}
+
+// --------------------------------------------------------- generator G
+// splitmix64 finaliser (Steele, Lea & Flood, OOPSLA 2014) as a counter hash;
+// h_a ~ N(0,1) by Box-Muller; U = exp(i scale sum_a h_a lambda_a/2).
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double unit_open(unsigned long long seed, unsigned long long ctr) {
+    const unsigned long long r = mix64(seed ^ mix64(ctr));
+    return ((double)(r >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+template <typename R>
+__global__ void k_generate_G(cplx<R>* __restrict__ U, int V, unsigned long long seed, double scale) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * V) return;
+    const int mu = t / V, s = t - mu * V;
+    const unsigned long long l = (unsigned long long)s * 4ull + (unsigned long long)mu;  // file-order link index
+    double h[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const unsigned long long c = l * 8ull + (unsigned long long)a;
+        const double u1 = unit_open(seed, 2ull * c), u2 = unit_open(seed, 2ull * c + 1ull);
+        h[a] = sqrt(-2.0 * log(u1)) * cos(6.28318530717958647692 * u2);
+    }
+    // X = i scale H,  H = sum_a h_a lambda_a / 2 ; coordinates of X:
+    // X00 = i s (h2/2 + h7/(2 sqrt3)), X11 = i s (-h2/2 + h7/(2 sqrt3)),
+    // X01 = i s (h0 - i h1)/2 = s (h1/2, h0/2), X02 = s (h4/2, h3/2), X12 = s (h6/2, h5/2)
+    const double is3 = 0.57735026918962576451;
+    alg<double> x;
+    x.v[0] = scale * (0.5 * h[2] + 0.5 * is3 * h[7]);
+    x.v[1] = scale * (-0.5 * h[2] + 0.5 * is3 * h[7]);
+    x.v[2] = scale * 0.5 * h[1];
+    x.v[3] = scale * 0.5 * h[0];
+    x.v[4] = scale * 0.5 * h[4];
+    x.v[5] = scale * 0.5 * h[3];
+    x.v[6] = scale * 0.5 * h[6];
+    x.v[7] = scale * 0.5 * h[5];
+    const su3<double> e = expm_alg<double>(x);
+    su3<R> o;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.m[k] = cmk<R>((R)e.m[k].re, (R)e.m[k].im);
+    store_link(U, V, mu, s, o);
+}
+
+// ------------------------------------------------------- reunitarisation
+// FP32-mixed form only: rows r0, r1 by Gram-Schmidt in double, r2 = conj(r0 x r1).
+template <typename R>
+__global__ void k_reunitarize(cplx<R>* __restrict__ U, int V) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * V) return;
+    const int mu = t / V, s = t - mu * V;
+    const su3<R> a = load_link(U, V, mu, s);
+    cplx<double> r0[3], r1[3], r2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r0[k] = cmk<double>(a.m[k].re, a.m[k].im);
+        r1[k] = cmk<double>(a.m[3 + k].re, a.m[3 + k].im);
+    }
+    double n0 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) n0 += r0[k].re * r0[k].re + r0[k].im * r0[k].im;
+    n0 = rsqrt(n0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r0[k] = cmk<double>(r0[k].re * n0, r0[k].im * n0);
+    cplx<double> d = cmk<double>(0.0, 0.0);  // <r0, r1> = sum conj(r0) r1
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d = ccfma(r0[k], r1[k], d);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r1[k] = csub(r1[k], cmul(d, r0[k]));
+    double n1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) n1 += r1[k].re * r1[k].re + r1[k].im * r1[k].im;
+    n1 = rsqrt(n1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r1[k] = cmk<double>(r1[k].re * n1, r1[k].im * n1);
+    // r2 = conj(r0 x r1)
+    r2[0] = csub(cmul(r0[1], r1[2]), cmul(r0[2], r1[1]));
+    r2[1] = csub(cmul(r0[2], r1[0]), cmul(r0[0], r1[2]));
+    r2[2] = csub(cmul(r0[0], r1[1]), cmul(r0[1], r1[0]));
+    su3<R> o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        o.m[k] = cmk<R>((R)r0[k].re, (R)r0[k].im);
+        o.m[3 + k] = cmk<R>((R)r1[k].re, (R)r1[k].im);
+        o.m[6 + k] = cmk<R>((R)r2[k].re, (R)(-r2[k].im));
+    }
+    store_link(U, V, mu, s, o);
+}
+
+// max over links of ||U^dag U - 1||_F (x) and |det U - 1| (y), per block
+template <typename R>
+__global__ void __launch_bounds__(256) k_unitarity(const cplx<R>* __restrict__ U, int V, double2* __restrict__ partial) {
+    __shared__ double su[256], sd[256];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double eu = 0.0, ed = 0.0;
+    if (t < 4 * V) {
+        const int mu = t / V, s = t - mu * V;
+        const su3<R> a = load_link(U, V, mu, s);
+        su3<double> b;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) b.m[k] = cmk<double>(a.m[k].re, a.m[k].im);
+        const su3<double> p = mul_an(b, b);
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const double re = p.m[k].re - ((k % 4) == 0 ? 1.0 : 0.0);
+            acc += re * re + p.m[k].im * p.m[k].im;
+        }
+        eu = sqrt(acc);
+        cplx<double> det = cmul(b.m[0], csub(cmul(b.m[4], b.m[8]), cmul(b.m[5], b.m[7])));
+        det = csub(det, cmul(b.m[1], csub(cmul(b.m[3], b.m[8]), cmul(b.m[5], b.m[6]))));
+        det = cadd(det, cmul(b.m[2], csub(cmul(b.m[3], b.m[7]), cmul(b.m[4], b.m[6]))));
+        ed = hypot(det.re - 1.0, det.im);
+    }
+    su[threadIdx.x] = eu;
+    sd[threadIdx.x] = ed;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            su[threadIdx.x] = fmax(su[threadIdx.x], su[threadIdx.x + w]);
+            sd[threadIdx.x] = fmax(sd[threadIdx.x], sd[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(su[0], sd[0]);
+}
+
+// ---------------------------------------------------- per-function debug
+template <typename R> __device__ __forceinline__ void store_alg_as_antiherm(double2* dst, const alg<R>& z) {
+    const double v0 = z.v[0], v1 = z.v[1];
+    dst[0] = make_double2(0.0, v0);
+    dst[4] = make_double2(0.0, v1);
+    dst[8] = make_double2(0.0, -(v0 + v1));
+    dst[1] = make_double2(z.v[2], z.v[3]);
+    dst[3] = make_double2(-(double)z.v[2], z.v[3]);
+    dst[2] = make_double2(z.v[4], z.v[5]);
+    dst[6] = make_double2(-(double)z.v[4], z.v[5]);
+    dst[5] = make_double2(z.v[6], z.v[7]);
+    dst[7] = make_double2(-(double)z.v[6], z.v[7]);
+}
+template <typename R> __device__ __forceinline__ void store_alg_as_herm(double2* dst, const alg<R>& f) {
+    const double v0 = f.v[0], v1 = f.v[1];
+    dst[0] = make_double2(v0, 0.0);
+    dst[4] = make_double2(v1, 0.0);
+    dst[8] = make_double2(-(v0 + v1), 0.0);
+    dst[1] = make_double2(f.v[2], f.v[3]);
+    dst[3] = make_double2(f.v[2], -(double)f.v[3]);
+    dst[2] = make_double2(f.v[4], f.v[5]);
+    dst[6] = make_double2(f.v[4], -(double)f.v[5]);
+    dst[5] = make_double2(f.v[6], f.v[7]);
+    dst[7] = make_double2(f.v[6], -(double)f.v[7]);
+}
+
+// flow gradient Z(x, mu) for every link, file order [s][mu][9] (double2)
+template <typename R>
+__global__ void k_debug_gradient(const cplx<R>* __restrict__ U, Geom g, double2* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    const int mu = t / g.V, s = t - mu * g.V;
+    const Coord c = site_coord(g, s);
+    su3<R> u;
+    const alg<R> Z = flow_gradient<R>(U, g, s, c, mu, u);
+    store_alg_as_antiherm(out + ((size_t)s * 4 + mu) * 9, Z);
+}
+
+// clover F and improved F for every (site, plane (01,02,03,12,13,23)), [s][p][9]
+template <typename R>
+__global__ void k_debug_fields(const cplx<R>* __restrict__ U, Geom g, double2* __restrict__ clover,
+                               double2* __restrict__ improved) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * g.V) return;
+    const int p = t / g.V, s = t - p * g.V;
+    const Coord c = site_coord(g, s);
+    alg<R> F11, Fh;
+    plane_fields<R>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], F11, Fh);
+    store_alg_as_herm(clover + ((size_t)s * 6 + p) * 9, F11);
+    store_alg_as_herm(improved + ((size_t)s * 6 + p) * 9, Fh);
+}
+
+// exp(iP) for n anti-Hermitian traceless matrices given as full 3x3 (double2)
+template <typename R>
+__global__ void k_debug_exp(const double2* __restrict__ in, double2* __restrict__ out, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double2* m = in + (size_t)t * 9;
+    alg<R> x;
+    x.v[0] = (R)m[0].y;
+    x.v[1] = (R)m[4].y;
+    x.v[2] = (R)m[1].x;
+    x.v[3] = (R)m[1].y;
+    x.v[4] = (R)m[2].x;
+    x.v[5] = (R)m[2].y;
+    x.v[6] = (R)m[5].x;
+    x.v[7] = (R)m[5].y;
+    const su3<R> e = expm_alg(x);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[(size_t)t * 9 + k] = make_double2(e.m[k].re, e.m[k].im);
+}
+
+}  // namespace lgf

@@ -1,0 +1,103 @@
+// Periodic 4-D lattice indexing and the device link layout.
+//
+// Replaces the reference's neighbour tables (LGF/Lattice/Lattice.cpp:190-230,
+// LGF/Field/Field.h:49-62) with index arithmetic: global site index
+// s = ((x0*N1 + x1)*N2 + x2)*N3 + x3 with x0 slowest (Lattice.cpp:423-436) and
+// periodic wrap in every direction (the "torus" type, Lattice.cpp:447-459).
+// One GPU holds the whole lattice, so there is no halo exchange.
+//
+// Device layout (structure of arrays, one complex entry per load):
+//   links  cplx<R>  U[(mu*9 + k) * V + s]        k = 3*row + col
+//   su(3)  R        A[(mu*8 + c) * V + s]        8 coordinates (lgf_su3.cuh)
+// so a warp of 32 consecutive sites reads 32 consecutive complex entries
+// (512 B for double, 256 B for float) per load instruction.
+#pragma once
+#include <stdint.h>
+#include "lgf_su3.cuh"
+
+namespace lgf {
+
+struct Geom {
+    int n[4];          // extents N0..N3
+    int stride[4];     // N1N2N3, N2N3, N3, 1
+    int V;             // total sites
+    int Vs;            // sites per x0 slice
+};
+
+inline Geom make_geom(const int shape[4]) {
+    Geom g;
+    for (int d = 0; d < 4; ++d) g.n[d] = shape[d];
+    g.stride[3] = 1;
+    g.stride[2] = shape[3];
+    g.stride[1] = shape[3] * shape[2];
+    g.stride[0] = shape[3] * shape[2] * shape[1];
+    g.Vs = g.stride[0];
+    g.V = g.stride[0] * shape[0];
+    return g;
+}
+
+struct Coord { int x[4]; };
+
+__device__ __forceinline__ Coord site_coord(const Geom& g, int s) {
+    Coord c;
+    unsigned r = (unsigned)s;
+    c.x[3] = (int)(r % (unsigned)g.n[3]); r /= (unsigned)g.n[3];
+    c.x[2] = (int)(r % (unsigned)g.n[2]); r /= (unsigned)g.n[2];
+    c.x[1] = (int)(r % (unsigned)g.n[1]); r /= (unsigned)g.n[1];
+    c.x[0] = (int)r;
+    return c;
+}
+
+// index of the neighbour of s (whose d-coordinate is xd) one step forward / back in d
+__device__ __forceinline__ int fwd(const Geom& g, int s, int d, int xd) {
+    return (xd == g.n[d] - 1) ? s - (g.n[d] - 1) * g.stride[d] : s + g.stride[d];
+}
+__device__ __forceinline__ int bwd(const Geom& g, int s, int d, int xd) {
+    return (xd == 0) ? s + (g.n[d] - 1) * g.stride[d] : s - g.stride[d];
+}
+__device__ __forceinline__ int wrap_inc(int x, int n) { return x == n - 1 ? 0 : x + 1; }
+__device__ __forceinline__ int wrap_dec(int x, int n) { return x == 0 ? n - 1 : x - 1; }
+
+template <typename R> struct vec2_of;
+template <> struct vec2_of<double> { typedef double2 type; };
+template <> struct vec2_of<float> { typedef float2 type; };
+
+template <typename R> __device__ __forceinline__ cplx<R> ldc(const cplx<R>* p) {
+    typedef typename vec2_of<R>::type V2;
+    V2 v = __ldg(reinterpret_cast<const V2*>(p));
+    return cmk<R>(v.x, v.y);
+}
+template <typename R> __device__ __forceinline__ void stc(cplx<R>* p, cplx<R> z) {
+    typedef typename vec2_of<R>::type V2;
+    V2 v;
+    v.x = z.re;
+    v.y = z.im;
+    *reinterpret_cast<V2*>(p) = v;
+}
+
+template <typename R> __device__ __forceinline__ su3<R> load_link(const cplx<R>* __restrict__ U, int V, int mu, int s) {
+    su3<R> a;
+    const cplx<R>* p = U + (size_t)mu * 9 * V + s;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a.m[k] = ldc(p + (size_t)k * V);
+    return a;
+}
+template <typename R> __device__ __forceinline__ void store_link(cplx<R>* __restrict__ U, int V, int mu, int s, const su3<R>& a) {
+    cplx<R>* p = U + (size_t)mu * 9 * V + s;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) stc(p + (size_t)k * V, a.m[k]);
+}
+template <typename R> __device__ __forceinline__ alg<R> load_alg(const R* __restrict__ A, int V, int mu, int s) {
+    alg<R> z;
+    const R* p = A + (size_t)mu * 8 * V + s;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) z.v[k] = __ldg(p + (size_t)k * V);
+    return z;
+}
+template <typename R> __device__ __forceinline__ void store_alg(R* __restrict__ A, int V, int mu, int s, const alg<R>& z) {
+    R* p = A + (size_t)mu * 8 * V + s;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) p[(size_t)k * V] = z.v[k];
+}
+
+}  // namespace lgf

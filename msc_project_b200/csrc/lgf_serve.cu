@@ -1,0 +1,355 @@
+// Continuous-batching flow server.
+//
+// A scheduler thread owns the context.  Each tick it (1) admits queued jobs in
+// arrival order while the head job's HBM footprint (links ring + RK3
+// accumulator + measurement buffers) fits the remaining budget and a slot is
+// free, (2) runs steps_per_tick RK3 steps of every resident job as shared
+// persistent launches (one group per precision, graph-captured once; the work
+// list and its length live in device memory so members join and leave without
+// re-capture), (3) measures the jobs that are due, and (4) retires finished
+// jobs: results are copied to the caller's arrays, device memory is released
+// and waiters are woken.  A job's arithmetic does not depend on which other
+// jobs share its launches, so its results are the same alone and in the mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "lgf_engine.cuh"
+
+using namespace lgf;
+
+namespace {
+
+struct ServeJob {
+    uint64_t id = 0;
+    lgf_job job{};
+    lgf_job_status st{};
+    size_t bytes = 0;
+    LatticeBuf buf;
+    int nmeas = 0;
+    int steps_done = 0;
+    double t = 0.0;
+    std::vector<double> tvals;
+};
+
+double now_s(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct lgf_server {
+    lgf_ctx* ctx = nullptr;
+    lgf_serve_config cfg{};
+    std::chrono::steady_clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServeJob*> queue;
+    std::map<uint64_t, std::unique_ptr<ServeJob>> jobs;
+    std::vector<ServeJob*> active;
+    size_t used = 0;
+    uint64_t next_id = 1;
+    bool stopping = false;
+    std::thread worker;
+    std::unique_ptr<GroupBase> group[2];
+    std::vector<LatticeBuf*> members[2];  // current member list of each group
+    std::vector<int> measured[2];         // current measured subset of each group
+    int threads[2] = {0, 0};
+    long long max_tiles[2] = {0, 0};
+    int fatal = LGF_OK;
+
+    void run();
+    int tick(std::vector<ServeJob*>& act);
+    int admit(ServeJob* j);
+    int retire(ServeJob* j);
+    void finish(ServeJob* j, int state, int err);
+};
+
+void lgf_server::finish(ServeJob* j, int state, int err) {
+    buf_free(j->buf);
+    std::lock_guard<std::mutex> lk(mu);
+    used -= j->bytes;
+    j->st.state = state;
+    j->st.error = err;
+    j->st.end_s = now_s(t0);
+    j->st.steps_done = j->steps_done;
+    cv_done.notify_all();
+}
+
+int lgf_server::admit(ServeJob* j) {
+    int rc = buf_alloc(ctx, j->buf, j->job.shape, j->job.precision, j->nmeas);
+    if (rc == LGF_OK)
+        rc = j->job.links ? upload_links(ctx, j->buf, j->job.links)
+                          : launch_generate(ctx, j->buf, j->job.seed, j->job.gen_scale);
+    if (rc != LGF_OK) return rc;
+    j->buf.eps = j->job.flow.eps;
+    j->t = j->job.flow.t0;
+    LGF_CUDA_TRY(ctx, cudaMemsetAsync(j->buf.slot, 0, sizeof(int), ctx->stream));
+    return LGF_OK;
+}
+
+int lgf_server::retire(ServeJob* j) {
+    lgf_job& jb = j->job;
+    if (j->nmeas > 0 && jb.meas) {
+        const int N0 = j->buf.g.n[0];
+        const size_t per = 2 + 2 * (size_t)N0;
+        std::vector<double> h(per * j->nmeas);
+        LGF_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), j->buf.meas, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        LGF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        for (int m = 0; m < j->nmeas; ++m) {
+            jb.meas->t[m] = j->tvals[m];
+            jb.meas->E[m] = h[m * per];
+            jb.meas->Q[m] = h[m * per + 1];
+            if (jb.meas->E_slice) std::memcpy(jb.meas->E_slice + (size_t)m * N0, &h[m * per + 2], N0 * sizeof(double));
+            if (jb.meas->Q_slice)
+                std::memcpy(jb.meas->Q_slice + (size_t)m * N0, &h[m * per + 2 + N0], N0 * sizeof(double));
+        }
+        jb.meas->count = j->nmeas;
+    } else if (jb.meas) {
+        jb.meas->count = 0;
+    }
+    if (jb.links_out) return download_links(ctx, j->buf, jb.links_out);
+    return LGF_OK;
+}
+
+// one scheduling tick over the resident jobs
+int lgf_server::tick(std::vector<ServeJob*>& act) {
+    std::vector<ServeJob*> byprec[2];
+    for (auto* j : act) byprec[j->job.precision].push_back(j);
+    for (int p = 0; p < 2; ++p) {
+        if (byprec[p].empty()) continue;
+        if (!group[p]) {
+            group[p].reset(make_group(ctx, p, threads[p], std::max(cfg.max_active, 1), max_tiles[p], true));
+            if (!group[p]) return LGF_ENOMEM;
+        }
+        std::vector<LatticeBuf*> m;
+        for (auto* j : byprec[p]) m.push_back(&j->buf);
+        int rc = LGF_OK;
+        if (m != members[p]) {
+            rc = group[p]->set_members(m);
+            if (rc != LGF_OK) return rc;
+            members[p] = m;
+            measured[p] = {-1};
+        }
+        auto measure = [&](const std::vector<int>& which) -> int {
+            if (which != measured[p]) {
+                int e = group[p]->set_measured(which);
+                if (e != LGF_OK) return e;
+                measured[p] = which;
+            }
+            return group[p]->replay_measure();
+        };
+        // measurements at t0 for newly admitted jobs
+        std::vector<int> which;
+        for (size_t i = 0; i < byprec[p].size(); ++i) {
+            ServeJob* j = byprec[p][i];
+            if (j->steps_done == 0 && j->job.flow.measure_at_t0 && j->tvals.empty()) {
+                which.push_back((int)i);
+                j->tvals.push_back(j->t);
+            }
+        }
+        if (!which.empty()) {
+            rc = measure(which);
+            if (rc != LGF_OK) return rc;
+        }
+        const int k = std::max(cfg.steps_per_tick, 1);
+        for (int s = 0; s < k; ++s) {
+            // members that already reached their step count leave the list
+            std::vector<ServeJob*> run;
+            for (auto* j : byprec[p])
+                if (j->steps_done < j->job.flow.nsteps) run.push_back(j);
+            if (run.empty()) break;
+            if (run.size() != byprec[p].size()) {
+                byprec[p] = run;
+                m.clear();
+                for (auto* j : run) m.push_back(&j->buf);
+                rc = group[p]->set_members(m);
+                if (rc != LGF_OK) return rc;
+                members[p] = m;
+                measured[p] = {-1};
+            }
+            rc = group[p]->replay_step();
+            if (rc != LGF_OK) return rc;
+            which.clear();
+            for (size_t i = 0; i < run.size(); ++i) {
+                ServeJob* j = run[i];
+                j->steps_done++;
+                j->t += j->job.flow.eps;  // GradientFlow.cpp:52
+                const lgf_flow_opts& o = j->job.flow;
+                if (p == LGF_PREC_FP32MIXED && o.reunit_every > 0 && j->steps_done % o.reunit_every == 0) {
+                    rc = launch_reunitarize(ctx, j->buf);
+                    if (rc != LGF_OK) return rc;
+                }
+                if (o.meas_every > 0 && j->steps_done % o.meas_every == 0) {
+                    which.push_back((int)i);
+                    j->tvals.push_back(j->t);
+                }
+            }
+            if (!which.empty()) {
+                rc = measure(which);
+                if (rc != LGF_OK) return rc;
+            }
+        }
+    }
+    return LGF_OK;
+}
+
+void lgf_server::run() {
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        std::vector<ServeJob*> admitted;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (active.empty() && queue.empty() && !stopping)
+                cv_work.wait_for(lk, std::chrono::milliseconds(20));
+            if (stopping) break;
+            // arrival-order admission by HBM footprint and free slots
+            while (!queue.empty() && (int)(active.size() + admitted.size()) < cfg.max_active &&
+                   used + queue.front()->bytes <= cfg.hbm_budget_bytes) {
+                ServeJob* j = queue.front();
+                queue.pop_front();
+                used += j->bytes;
+                j->st.state = LGF_JOB_RUNNING;
+                j->st.start_s = now_s(t0);
+                admitted.push_back(j);
+            }
+        }
+        for (auto* j : admitted) {
+            int rc = admit(j);
+            if (rc != LGF_OK) finish(j, LGF_JOB_FAILED, rc);
+            else active.push_back(j);
+        }
+        if (active.empty()) continue;
+        int rc = tick(active);
+        if (rc != LGF_OK) {
+            for (auto* j : active) finish(j, LGF_JOB_FAILED, rc);
+            active.clear();
+            continue;
+        }
+        std::vector<ServeJob*> keep;
+        for (auto* j : active) {
+            if (j->steps_done >= j->job.flow.nsteps) {
+                int r2 = retire(j);
+                finish(j, r2 == LGF_OK ? LGF_JOB_DONE : LGF_JOB_FAILED, r2);
+            } else {
+                keep.push_back(j);
+            }
+        }
+        active.swap(keep);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    for (auto* j : active) finish(j, LGF_JOB_FAILED, LGF_ESHUTDOWN);
+    active.clear();
+    group[0].reset();
+    group[1].reset();
+}
+
+extern "C" {
+
+int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out) {
+    if (!ctx || !cfg || !out) return LGF_EINVAL;
+    *out = nullptr;
+    if (cfg->max_active < 1 || cfg->hbm_budget_bytes == 0) return set_error(ctx, LGF_EINVAL, "empty serve budget");
+    cudaSetDevice(ctx->device);
+    lgf_server* s = new (std::nothrow) lgf_server();
+    if (!s) return LGF_ENOMEM;
+    s->ctx = ctx;
+    s->cfg = *cfg;
+    if (s->cfg.steps_per_tick < 1) s->cfg.steps_per_tick = 1;
+    s->t0 = std::chrono::steady_clock::now();
+    for (int p = 0; p < 2; ++p) {
+        s->threads[p] = ctx->tuned_threads[p] ? ctx->tuned_threads[p] : default_threads(p);
+        // the budget bounds the resident sites: every site costs at least its links ring + accumulator
+        const size_t per_site = (p == 0 ? 8 : 4) * (3 * 4 * 18 + 4 * 8);
+        const long long max_sites = (long long)(cfg->hbm_budget_bytes / per_site) + 1;
+        s->max_tiles[p] = (4 * max_sites) / s->threads[p] + 2LL * cfg->max_active + 1;
+    }
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return LGF_OK;
+}
+
+int lgf_serve_submit(lgf_server* s, const lgf_job* job, uint64_t* id) {
+    if (!s || !job || !id) return LGF_EINVAL;
+    if (!valid_shape(job->shape) || (job->precision != LGF_PREC_FP64 && job->precision != LGF_PREC_FP32MIXED) ||
+        job->flow.nsteps < 0 || job->flow.meas_every < 0 || job->flow.reunit_every < 0 || job->shape[0] > 256)
+        return LGF_EINVAL;
+    const int nm = count_measurements(job->flow);
+    if (nm > 0 && (!job->meas || !job->meas->t || !job->meas->E || !job->meas->Q || job->meas->capacity < nm))
+        return LGF_EINVAL;
+    auto j = std::make_unique<ServeJob>();
+    j->job = *job;
+    j->nmeas = nm;
+    j->bytes = footprint_bytes(job->shape, job->precision, nm);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return LGF_ESHUTDOWN;
+    if (j->bytes > s->cfg.hbm_budget_bytes) return LGF_ENOMEM;  // could never be admitted
+    j->id = s->next_id++;
+    j->st.state = LGF_JOB_QUEUED;
+    j->st.submit_s = now_s(s->t0);
+    *id = j->id;
+    s->queue.push_back(j.get());
+    s->jobs[j->id] = std::move(j);
+    s->cv_work.notify_all();
+    return LGF_OK;
+}
+
+int lgf_serve_poll(lgf_server* s, uint64_t id, lgf_job_status* st) {
+    if (!s) return LGF_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return LGF_ENOTFOUND;
+    if (st) {
+        *st = it->second->st;
+        st->steps_done = it->second->steps_done;
+    }
+    const int state = it->second->st.state;
+    return (state == LGF_JOB_DONE || state == LGF_JOB_FAILED) ? LGF_OK : LGF_EBUSY;
+}
+
+int lgf_serve_wait(lgf_server* s, uint64_t id, double timeout_s, lgf_job_status* st) {
+    if (!s) return LGF_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return LGF_ENOTFOUND;
+    ServeJob* j = it->second.get();
+    auto done = [&] { return j->st.state == LGF_JOB_DONE || j->st.state == LGF_JOB_FAILED; };
+    if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(std::max(timeout_s, 0.0)), done)) {
+        if (st) *st = j->st;
+        return LGF_ETIMEDOUT;
+    }
+    if (st) *st = j->st;
+    return LGF_OK;
+}
+
+int lgf_serve_stop(lgf_server* s) {
+    if (!s) return LGF_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        for (auto* j : s->queue) {
+            j->st.state = LGF_JOB_FAILED;
+            j->st.error = LGF_ESHUTDOWN;
+            j->st.end_s = now_s(s->t0);
+        }
+        s->queue.clear();
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    s->cv_done.notify_all();
+    delete s;
+    return LGF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+"""Generate the golden fixtures under tests/golden/ from the LGF reference itself.
+
+Runs oracle/_ref/lgf_ref (the unmodified reference sources compiled by
+oracle/Makefile with the single-rank MPI stub and the seed shim) and writes:
+
+  hb8_seed1.bin            config 1 input: reference heatbath, beta=6.0, seed 1,
+                           8^4, 200 x (Cabibbo-Marinari + 5 OR) sweeps, saved
+                           configuration #0 (reference file layout, 2.36 MB)
+  flow8_hb_seed1.json      FlowSavedGaugeConfigurations on it: eps=0.01, 100
+                           steps, E(t), Q(t) every step at 17 digits (stdout),
+                           the reference's two CSV files verbatim, and the
+                           SHA-256 + a sample of the flowed configuration
+  g4466_seed7.bin          generator-G input (4x4x6x6, seed 7, scale 0.5)
+  kernels_g4466.npz        per-function reference outputs on it (staple, flow
+                           gradient, clover F, improved F, e(x), q(x), one RK3
+                           step) for every 5th site
+  flow_g4466.json          FlowSavedGaugeConfigurations on it: 20 steps, meas every 5
+  exp_cases.npz            HermTrLessExp on 512 matrices spanning both branches
+  flow16_g7.json           16^4 generator-G seed 7: 10 steps, measure every 5
+
+Usage:  python tests/golden/make_golden.py [--skip-heatbath] [--skip-16]
+The heatbath takes ~3 min and the 8^4 flow ~1.5 min on one core.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+from oracle import oracle as O  # noqa: E402
+
+BETA_DIR = "beta6_000000"
+
+
+def shape_dir(shape):
+    return "X".join(str(s) for s in shape)
+
+
+def run_ref(args, **kw):
+    return O.run_reference(args, **kw)
+
+
+def parse_stdout(text):
+    Q = [float(m) for m in re.findall(r"Topological Charge = (\S+)", text)]
+    E = [float(m) for m in re.findall(r"Energy Density\s*= (\S+)", text)]
+    return E, Q
+
+
+def reference_flow(work: Path, links: np.ndarray, shape, steps, eps, meas):
+    """Place links under the reference's hard-coded input tag and run
+    FlowSavedGaugeConfigurations (LGF/LGF.cpp:163-196) for configuration 0."""
+    d = work / "ensembles" / "su3" / BETA_DIR / shape_dir(shape) / "LHMC_3_of_0_330000"
+    d.mkdir(parents=True, exist_ok=True)
+    links.astype(np.float64).tofile(d / "torus_extdof4_0.bin")
+    out = run_ref(["flow", str(work) + "/", "6.0", *shape, 0, 0, steps, eps, meas])
+    E, Q = parse_stdout(out.stdout)
+    obs = work / "Observables"
+    csv_q = (obs / "Topological_Charge" / BETA_DIR / shape_dir(shape) / "GF" / "torus_extdof4_0.csv").read_text()
+    csv_e = (obs / "EnergyDensity" / BETA_DIR / shape_dir(shape) / "GF" / "torus_extdof4_0.csv").read_text()
+    flowed_dir = work / "ensembles" / "su3" / BETA_DIR / shape_dir(shape) / "GF"
+    files = sorted(flowed_dir.glob("*.bin"))
+    flowed = np.fromfile(files[0]) if files else None
+    return E, Q, csv_e, csv_q, files[0].name if files else None, flowed
+
+
+def times(n_meas, eps, meas):
+    t, out = 0.0, [0.0]
+    for s in range(1, (n_meas - 1) * meas + 1):
+        t += eps
+        if s % meas == 0:
+            out.append(t)
+    return out
+
+
+def write_flow_json(path, shape, steps, eps, meas, input_name, E, Q, csv_e, csv_q, fname, flowed):
+    rec = {
+        "shape": list(shape), "beta": 6.0, "eps": eps, "steps": steps, "meas_every": meas,
+        "input": input_name,
+        "t": times(len(E), eps, meas), "E": E, "Q": Q,
+        "csv_energy": csv_e, "csv_topcharge": csv_q,
+        "flowed_file": fname,
+        "flowed_sha256": hashlib.sha256(flowed.tobytes()).hexdigest() if flowed is not None else None,
+        "flowed_sample": flowed[: 4 * 18 * 2].tolist() if flowed is not None else None,
+        "generator": "oracle/_ref/lgf_ref (unmodified LGF sources) via tests/golden/make_golden.py",
+    }
+    path.write_text(json.dumps(rec, indent=1))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--skip-heatbath", action="store_true")
+    ap.add_argument("--skip-16", action="store_true")
+    args = ap.parse_args()
+    O.build()
+    if not O.reference_available():
+        sys.exit("reference harness not built: the reference tree is needed to make fixtures")
+    with tempfile.TemporaryDirectory() as tmp:
+        tmp = Path(tmp)
+        # ---- config 1: heatbath input + 8^4 flow
+        hb = HERE / "hb8_seed1.bin"
+        if not args.skip_heatbath or not hb.exists():
+            run_ref(["heatbath", str(tmp / "hb") + "/", "6.0", 8, 8, 8, 8, 200, 5], env={"LGF_REF_SEED": "1"})
+            src = tmp / "hb" / "ensembles" / "su3" / BETA_DIR / "8X8X8X8" / "Heatbath_5_ORperHB" / "torus_extdof4_0.bin"
+            shutil.copy(src, hb)
+        links = np.fromfile(hb)
+        res = reference_flow(tmp / "f8", links, (8, 8, 8, 8), 100, 0.01, 1)
+        write_flow_json(HERE / "flow8_hb_seed1.json", (8, 8, 8, 8), 100, 0.01, 1, hb.name, *res)
+
+        # ---- small generator-G lattice: per-function outputs and a short flow
+        shape = (4, 4, 6, 6)
+        g = O.generate_G(shape, 7, 0.5)
+        g.tofile(HERE / "g4466_seed7.bin")
+        run_ref(["kernels", HERE / "g4466_seed7.bin", *shape, str(tmp / "k_")])
+        V = O.volume(shape)
+        sites = np.arange(0, V, 5)
+        fields = {}
+        for name, per in (("staple", 4), ("grad", 4), ("clover", 6), ("improved", 6), ("rk3step", 4)):
+            a = np.fromfile(tmp / f"k_{name}.bin").reshape(V, per, 18)
+            fields[name] = a[sites]
+        for name in ("edens", "qdens"):
+            fields[name] = np.fromfile(tmp / f"k_{name}.bin")[sites]
+        np.savez(HERE / "kernels_g4466.npz", sites=sites, shape=np.array(shape), **fields)
+        res = reference_flow(tmp / "fg", g, shape, 20, 0.01, 5)
+        write_flow_json(HERE / "flow_g4466.json", shape, 20, 0.01, 5, "g4466_seed7.bin", *res)
+
+        # ---- exponential on both Cayley-Hamilton branches
+        rng = np.random.default_rng(2024)
+        n = 512
+        H = rng.normal(size=(n, 3, 3)) + 1j * rng.normal(size=(n, 3, 3))
+        H = (H + np.conj(np.transpose(H, (0, 2, 1)))) / 2
+        H -= np.trace(H, axis1=1, axis2=2)[:, None, None] / 3 * np.eye(3)
+        scale = np.exp(rng.uniform(np.log(1e-4), np.log(3.0), size=n))[:, None, None]
+        iP = np.ascontiguousarray(1j * H * scale)
+        iP.view(np.float64).tofile(tmp / "iP.bin")
+        run_ref(["exp", tmp / "iP.bin", tmp / "eo.bin"])
+        np.savez(HERE / "exp_cases.npz", iP=iP.view(np.float64).reshape(n, 18),
+                 exp=np.fromfile(tmp / "eo.bin").reshape(n, 18))
+
+        # ---- 16^4 generator G, seed 7 (throughput-config lattice), short flow
+        if not args.skip_16:
+            shape = (16, 16, 16, 16)
+            g16 = O.generate_G(shape, 7, 0.5)
+            res = reference_flow(tmp / "f16", g16, shape, 10, 0.01, 5)
+            write_flow_json(HERE / "flow16_g7.json", shape, 10, 0.01, 5, "generator G seed 7 scale 0.5", *res)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

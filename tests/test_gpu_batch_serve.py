@@ -1,0 +1,84 @@
+"""Batched and served forms: every job's result is the same alone and in the
+mix (bit for bit: a job's arithmetic does not depend on its neighbours in the
+shared launches), admission respects the HBM budget, and errors are reported."""
+import time
+
+import numpy as np
+import pytest
+from conftest import golden_links
+
+from msc_project_b200 import FP32MIXED, FP64, Job, LGFError, Server
+from msc_project_b200 import _capi as C
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(ctx, job: Job):
+    with ctx.lattice(job.shape, job.precision) as lat:
+        if job.links is not None:
+            lat.upload(job.links)
+        else:
+            lat.generate(job.seed, job.gen_scale)
+        r = lat.flow(job.eps, job.nsteps, job.meas_every, job.t0, job.measure_at_t0, job.reunit_every)
+        return r, lat.download()
+
+
+def mixed_jobs():
+    return [
+        Job((8, 8, 8, 8), FP64, links=golden_links("hb8_seed1.bin"), nsteps=12, meas_every=4, want_links=True),
+        Job((4, 4, 6, 6), FP64, seed=101, nsteps=7, meas_every=2, want_links=True),
+        Job((6, 6, 6, 12), FP64, seed=102, nsteps=10, meas_every=5, want_links=True),
+        Job((8, 8, 8, 8), FP32MIXED, seed=103, nsteps=12, meas_every=3, reunit_every=5, want_links=True),
+        Job((4, 8, 8, 8), FP32MIXED, seed=104, nsteps=5, meas_every=5, want_links=True),
+    ]
+
+
+def test_batch_equals_alone(ctx):
+    jobs = mixed_jobs()
+    st = ctx.batch_run(jobs)
+    assert st.site_steps == sum(np.prod(j.shape) * j.nsteps for j in jobs)
+    assert st.seconds > 0 and st.launches > 0 and st.block_threads in (64, 128, 256)
+    for j in jobs:
+        r, links = alone(ctx, Job(**{k: getattr(j, k) for k in ("shape", "precision", "links", "seed", "nsteps",
+                                                                     "meas_every", "reunit_every")}))
+        assert np.array_equal(j.result.t, r.t)
+        assert np.array_equal(j.result.E, r.E), j.shape
+        assert np.array_equal(j.result.Q, r.Q), j.shape
+        assert np.array_equal(j.links_out, links)
+
+
+def test_autotune_picks_a_candidate(ctx):
+    assert ctx.autotune(FP64, (8, 8, 8, 16)) in (64, 128, 256)
+
+
+def test_server_alone_vs_mix_and_latency(ctx):
+    jobs = mixed_jobs()
+    refs = [alone(ctx, Job(**{k: getattr(j, k) for k in ("shape", "precision", "links", "seed", "nsteps",
+                                                            "meas_every", "reunit_every")})) for j in jobs]
+    # budget for about two resident jobs: the rest queue and are admitted as memory frees up
+    budget = 2 * ctx.lib.lgf_lattice_footprint((C.ctypes.c_int * 4)(8, 8, 8, 8), FP64) + (1 << 20)
+    with Server(ctx, budget, max_active=4, steps_per_tick=1) as srv:
+        ids = []
+        for j in jobs:
+            ids.append(srv.submit(j))
+            time.sleep(0.005)
+        sts = [srv.wait(i, 120.0) for i in ids]
+    for j, st, (r, links) in zip(jobs, sts, refs):
+        assert st.state == C.LGF_JOB_DONE and st.error == 0
+        assert st.submit_s <= st.start_s <= st.end_s
+        assert np.array_equal(j.result.E, r.E) and np.array_equal(j.result.Q, r.Q)
+        assert np.array_equal(j.links_out, links)
+    lat = np.array([s.end_s - s.submit_s for s in sts])
+    assert np.percentile(lat, 99) >= np.percentile(lat, 50) > 0
+
+
+def test_server_rejects_jobs_that_never_fit(ctx):
+    with Server(ctx, 1 << 20, max_active=2) as srv:
+        with pytest.raises(LGFError) as e:
+            srv.submit(Job((8, 8, 8, 8), FP64, seed=1, nsteps=1))
+        assert e.value.code == C.LGF_ENOMEM
+        with pytest.raises(LGFError) as e:
+            srv.submit(Job((8, 8, 7, 8), FP64, seed=1, nsteps=1))
+        assert e.value.code == C.LGF_EINVAL
+        rc, _ = srv.poll(12345)
+        assert rc == C.LGF_ENOTFOUND

@@ -1,0 +1,273 @@
+"""GPU parity: the CUDA engine through the C ABI against the reference's golden
+vectors and the CPU oracle, plus size-independent properties.
+
+Tolerances (FP64 plain form): E relative 1e-12; Q as |dQ| <= 1e-12 max(1,|Q|);
+links 1e-12 absolute.  The kernels use fused multiply-adds and another
+summation order than the reference, so agreement is to rounding, not bitwise.
+FP32-mixed form: |dQ| < 1e-3, |dE|/E < 1e-5 against FP64.
+"""
+import hashlib
+import os
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+from conftest import GOLDEN, golden_json, golden_links, q_err, rel_err
+
+from msc_project_b200 import FP32MIXED, FP64, Job
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def as_mats(a, per):
+    return np.asarray(a).reshape(-1, per, 18)
+
+
+# ------------------------------------------------------------ per function
+def test_exp_against_reference(ctx):
+    z = np.load(GOLDEN / "exp_cases.npz")
+    out = ctx.exp_su3(z["iP"], FP64).reshape(-1, 18)
+    assert np.max(np.abs(out - z["exp"])) < 1e-13
+    out32 = ctx.exp_su3(z["iP"], FP32MIXED).reshape(-1, 18)
+    assert np.max(np.abs(out32 - z["exp"])) < 5e-6
+
+
+def test_exp_zero_is_identity(ctx):
+    out = ctx.exp_su3(np.zeros((3, 18)), FP64).reshape(-1, 9, 2)
+    assert np.array_equal(out[:, :, 0], np.tile(np.eye(3).reshape(9), (3, 1)))
+    assert not out[:, :, 1].any()
+
+
+def test_kernels_against_reference(ctx):
+    k = np.load(GOLDEN / "kernels_g4466.npz")
+    shape = tuple(int(s) for s in k["shape"])
+    sites = k["sites"]
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(golden_links("g4466_seed7.bin"))
+        grad = as_mats(lat.debug_gradient(), 4)
+        assert np.max(np.abs(grad[sites] - k["grad"])) < 1e-13
+        clov, impr = lat.debug_fields()
+        assert np.max(np.abs(as_mats(clov, 6)[sites] - k["clover"])) < 1e-13
+        assert np.max(np.abs(as_mats(impr, 6)[sites] - k["improved"])) < 1e-13
+        e, q = lat.site_densities()
+        assert np.max(np.abs(e[sites] - k["edens"])) < 1e-12
+        assert np.max(np.abs(q[sites] - k["qdens"])) < 1e-12
+        lat.flow(0.01, 1, 0, measure_at_t0=False)
+        after = as_mats(lat.download(), 4)
+        assert np.max(np.abs(after[sites] - k["rk3step"])) < 1e-13
+
+
+def test_generator_matches_oracle(ctx):
+    shape = (4, 4, 6, 6)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.generate(7, 0.5)
+        g = lat.download()
+    assert np.max(np.abs(g - golden_links("g4466_seed7.bin"))) < 1e-13
+
+
+def test_upload_download_roundtrip(ctx):
+    U = golden_links("hb8_seed1.bin")
+    with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+        lat.upload(U)
+        assert np.array_equal(lat.download(), U)
+
+
+# ------------------------------------------------------------- end to end
+@pytest.mark.parametrize("name,inp", [("flow_g4466.json", "g4466_seed7.bin"),
+                                      ("flow8_hb_seed1.json", "hb8_seed1.bin")])
+def test_flow_against_reference(ctx, name, inp):
+    g = golden_json(name)
+    with ctx.lattice(g["shape"], FP64) as lat:
+        lat.upload(golden_links(inp))
+        r = lat.flow(g["eps"], g["steps"], g["meas_every"])
+        Uf = lat.download()
+    assert np.allclose(r.t, g["t"], rtol=0, atol=1e-12)
+    assert rel_err(r.E, g["E"]) < TOL
+    assert q_err(r.Q, g["Q"]) < TOL
+    assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < TOL
+
+
+def test_flow8_links_against_oracle(ctx):
+    U = golden_links("hb8_seed1.bin")
+    shape = (8, 8, 8, 8)
+    _, _, _, Uo = O.flow(U, shape, 0.01, 100, 0)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        lat.flow(0.01, 100, 0, measure_at_t0=False)
+        Ug = lat.download()
+    assert np.max(np.abs(Ug - Uo)) < TOL
+
+
+def test_flow16_against_reference(ctx):
+    g = golden_json("flow16_g7.json")
+    with ctx.lattice(g["shape"], FP64) as lat:
+        lat.generate(7, 0.5)
+        r = lat.flow(g["eps"], g["steps"], g["meas_every"])
+    # device-generated inputs differ from the host file by rounding only
+    assert rel_err(r.E, g["E"]) < 1e-11
+    assert q_err(r.Q, g["Q"]) < 1e-11
+
+
+def test_dropin_flow_saved_matches_reference_outputs(ctx, tmp_path):
+    """FlowSavedGaugeConfigurations end to end: same input tree, same CSV bytes,
+    same flowed-file name, links within tolerance of the reference's."""
+    from msc_project_b200 import FlowParameters, FlowSavedGaugeConfigurations, SimulationParameters, configure
+    g = golden_json("flow8_hb_seed1.json")
+    folder = str(tmp_path) + "/"
+    d = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/LHMC_3_of_0_330000"
+    d.mkdir(parents=True)
+    (d / "torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
+    configure(FP64)
+    rc = FlowSavedGaugeConfigurations(SimulationParameters(4, 4, [8, 8, 8, 8], 6.0, [0, 0, 0, 0]),
+                                      FlowParameters(0, 0, 100, 0.01, 1, folder))
+    assert rc == 0
+    obs = tmp_path / "Observables"
+    csv_q = (obs / "Topological_Charge/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text()
+    csv_e = (obs / "EnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text()
+    assert csv_q == g["csv_topcharge"]
+    assert csv_e == g["csv_energy"]
+    flowed = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/GF" / g["flowed_file"]
+    Uf = np.fromfile(flowed)
+    assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < TOL
+
+
+def test_resume_continues_the_flow(ctx, tmp_path):
+    """Flowing 50 + resume 50 equals flowing 100 (ResumeFlowedConfiguration)."""
+    from msc_project_b200 import (FlowParameters, FlowSavedGaugeConfigurations, ResumeFlowedConfiguration,
+                                  SimulationParameters, configure)
+    configure(FP64)
+    folder = str(tmp_path) + "/"
+    d = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/LHMC_3_of_0_330000"
+    d.mkdir(parents=True)
+    (d / "torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
+    p = SimulationParameters(4, 4, [8, 8, 8, 8], 6.0, [0, 0, 0, 0])
+    assert FlowSavedGaugeConfigurations(p, FlowParameters(0, 0, 50, 0.01, 10, folder)) == 0
+    gf = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/GF"
+    assert (gf / "torus_extdof4_0_Flowtime0.500000.bin").exists()
+    assert ResumeFlowedConfiguration(p, FlowParameters(0, 0, 50, 0.01, 10, folder), 0.5) == 0
+    g = golden_json("flow8_hb_seed1.json")
+    Uf = np.fromfile(gf / "torus_extdof4_0_Flowtime1.000000.bin")
+    assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < 1e-11
+    rows = (tmp_path / "Observables/EnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text().split()
+    assert len(rows) == 6 + 5  # t=0 and every 10th of 50, then 5 more after the resume
+
+
+def test_qdensity_output(ctx, tmp_path):
+    from msc_project_b200 import FlowParameters, MeasureQdensityDistribution, SimulationParameters, configure
+    configure(FP64)
+    folder = str(tmp_path) + "/"
+    gf = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/GF"
+    gf.mkdir(parents=True)
+    U = golden_links("hb8_seed1.bin")
+    U.tofile(gf / "torus_extdof4_0_Flowtime1.000000.bin")
+    assert MeasureQdensityDistribution(SimulationParameters(4, 4, [8, 8, 8, 8], 6.0, [0, 0, 0, 0]),
+                                       FlowParameters(0, 0, 100, 0.01, 1, folder)) == 0
+    q = np.fromfile(tmp_path / "Observables/Qdensity/beta6_000000/8X8X8X8/GF/torus_extdof1_0_Flowtime1.000000.bin")
+    _, qo = O.site_densities(U, (8, 8, 8, 8))
+    assert q.shape == (8 ** 4,)
+    assert np.max(np.abs(q - (np.pi ** 2 / 4) * qo)) < 1e-11  # the reference's pi^2/4 prefactor
+
+
+# ------------------------------------------------------------- properties
+def random_gauge(U, shape, seed):
+    """U'_mu(x) = g(x) U_mu(x) g(x+mu)^dag with random SU(3) g (host numpy)."""
+    V = O.volume(shape)
+    g = O.generate_G(shape, seed, 1.0).reshape(V, 4, 18)[:, 0]
+    G = g[:, 0::2] + 1j * g[:, 1::2]
+    G = G.reshape(V, 3, 3)
+    M = (U.reshape(V, 4, 18)[:, :, 0::2] + 1j * U.reshape(V, 4, 18)[:, :, 1::2]).reshape(V, 4, 3, 3)
+    idx = np.arange(V).reshape(shape)
+    out = np.empty_like(M)
+    for mu in range(4):
+        nb = np.roll(idx, -1, axis=mu).reshape(-1)
+        out[:, mu] = G @ M[:, mu] @ np.conj(np.transpose(G[nb], (0, 2, 1)))
+    r = np.empty((V, 4, 9, 2))
+    r[..., 0] = out.reshape(V, 4, 9).real
+    r[..., 1] = out.reshape(V, 4, 9).imag
+    return r.reshape(-1)
+
+
+def test_gauge_invariance_and_parity(ctx):
+    shape = (8, 8, 8, 8)
+    U = golden_links("hb8_seed1.bin")
+    Ug = random_gauge(U, shape, 99)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        r1 = lat.flow(0.01, 20, 10)
+        lat.upload(Ug)
+        r2 = lat.flow(0.01, 20, 10)
+    assert rel_err(r2.E, r1.E) < 1e-11
+    assert q_err(r2.Q, r1.Q) < 1e-11
+
+
+def test_cold_start_stays_trivial(ctx):
+    shape = (4, 4, 4, 8)
+    V = O.volume(shape)
+    U = np.zeros((V, 4, 9, 2))
+    U[:, :, [0, 4, 8], 0] = 1.0
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U.reshape(-1))
+        r = lat.flow(0.01, 5, 1)
+        assert np.max(np.abs(lat.download() - U.reshape(-1))) < 1e-15
+    assert np.max(np.abs(r.E)) < 1e-28 and np.max(np.abs(r.Q)) < 1e-28
+
+
+def test_timeslices_sum_to_totals(ctx):
+    shape = (8, 8, 8, 8)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(golden_links("hb8_seed1.bin"))
+        r = lat.flow(0.01, 10, 5, slices=True)
+    assert np.allclose(r.E_slice.mean(axis=1), r.E, rtol=1e-13)
+    assert np.allclose(r.Q_slice.sum(axis=1), r.Q, rtol=0, atol=1e-12)
+
+
+def test_unitarity_after_flow(ctx):
+    with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+        lat.upload(golden_links("hb8_seed1.bin"))
+        lat.flow(0.01, 100, 0, measure_at_t0=False)
+        u, d = lat.unitarity()
+    assert u < 1e-13 and d < 1e-13
+
+
+def test_runs_are_deterministic(ctx):
+    outs = []
+    for _ in range(2):
+        with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+            lat.upload(golden_links("hb8_seed1.bin"))
+            r = lat.flow(0.01, 10, 5)
+            outs.append((r.E.copy(), r.Q.copy(), lat.download()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
+
+
+# ----------------------------------------------------------- FP32-mixed
+def test_fp32_mixed_accuracy(ctx):
+    shape = (8, 8, 8, 8)
+    U = golden_links("hb8_seed1.bin")
+    g = golden_json("flow8_hb_seed1.json")
+    with ctx.lattice(shape, FP32MIXED) as lat:
+        lat.upload(U)
+        r = lat.flow(0.01, 100, 1, reunit_every=10)
+        u, d = lat.unitarity()
+    assert q_err(r.Q, g["Q"]) < 1e-3
+    assert rel_err(r.E, g["E"]) < 1e-5
+    assert u < 1e-5 and d < 1e-5
+
+
+# ----------------------------------------------------- errors at the ABI
+def test_invalid_arguments(ctx):
+    from msc_project_b200 import LGFError
+    with pytest.raises(LGFError):
+        ctx.lattice((8, 8, 7, 8))
+    import ctypes
+    from msc_project_b200 import _capi as C
+    h = ctypes.c_void_p()
+    assert ctx.lib.lgf_lattice_create(ctx.h, (ctypes.c_int * 4)(8, 8, 8, 8), 5, ctypes.byref(h)) == C.LGF_EINVAL
+    assert "precision" in ctx.error()
+    with ctx.lattice((4, 4, 4, 4), FP64) as lat:
+        with pytest.raises(ValueError):
+            lat.upload(np.zeros(10))
