@@ -39,6 +39,7 @@ extern "C" {
 #define LGF_ENOTFOUND (-6)  /* unknown job id */
 #define LGF_EBUSY (-7)      /* result not ready yet */
 #define LGF_ESHUTDOWN (-8)  /* server stopped */
+#define LGF_ETOOBIG (-9)    /* size beyond the fixed maximum of lgf_measure_noalloc */
 
 #define LGF_PREC_FP64 0       /* the plain form: links and arithmetic in float64 */
 #define LGF_PREC_FP32MIXED 1  /* float32 links/RK3; float64 CH coefficients, reductions */
@@ -126,6 +127,24 @@ int lgf_profile_kernels(lgf_lattice* lat, double eps, int nrep, double ms[4]);
 /* Device seconds (CUDA events on the engine's stream) of the step and
  * measurement launches of the last lgf_flow call on this lattice. */
 int lgf_last_flow_seconds(lgf_lattice* lat, double* seconds);
+
+/* E and Q of a configuration that is already in device memory, without
+ * allocating any device memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code whose GPU memory is owned by
+ * another allocator (a framework's caching pool, a server that reserves all
+ * memory at start-up) or a loop that must never enter the driver's allocator.
+ *   links   device pointer, 16-byte aligned, float64 in file order (V*4*18)
+ *   out     device pointer, 2 + 2*N0 doubles: [E, Q, E_slice[N0], Q_slice[N0]]
+ *   stream  the cudaStream_t to launch on (NULL = legacy default stream)
+ * The launches are asynchronous on that stream; out is valid once it completes.
+ * Scratch is a fixed device array inside the library (4 MiB + 4 KiB per GPU,
+ * held until exit): N0 <= 256 and N0 * ceil(N1*N2*N3/32) <= 262144 (48^4 fits,
+ * 64^4 does not); larger lattices return LGF_ETOOBIG.  The first call on a
+ * device looks up the array's device address, so make it before any stream
+ * capture.  Calls share the array: calls that may overlap on one GPU (other
+ * streams, other host threads) race and must be ordered by the caller. */
+int lgf_measure_noalloc(const double* links, const int shape[4], double* out, void* stream);
 
 /* ------------------------------------------------------------------ batch */
 /* A flow job: one configuration, its flow schedule and its result arrays. */

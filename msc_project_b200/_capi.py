@@ -18,6 +18,7 @@ LGF_ETIMEDOUT = -5
 LGF_ENOTFOUND = -6
 LGF_EBUSY = -7
 LGF_ESHUTDOWN = -8
+LGF_ETOOBIG = -9
 
 LGF_PREC_FP64 = 0
 LGF_PREC_FP32MIXED = 1
@@ -80,6 +81,7 @@ SIGNATURES = {
     "lgf_exp_su3": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, ctypes.c_longlong]),
     "lgf_profile_kernels": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _dp]),
     "lgf_last_flow_seconds": (ctypes.c_int, [_vp, _dp]),
+    "lgf_measure_noalloc": (ctypes.c_int, [_dp, _ip, _dp, _vp]),
     "lgf_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_job), ctypes.c_int, ctypes.POINTER(lgf_batch_stats)]),
     "lgf_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip]),
     "lgf_serve_start": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_serve_config), ctypes.POINTER(_vp)]),
