@@ -197,6 +197,124 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------- forms
+def _flow_timed(ctx, lat, eps, nsteps, meas, reunit=0):
+    r = lat.flow(eps, nsteps, meas, 0.0, True, reunit)
+    secs = ctypes.c_double()
+    ctx.check(ctx.lib.lgf_last_flow_seconds(lat.h, ctypes.byref(secs)))
+    return r, secs.value
+
+
+def form_fp32mixed(ctx):
+    """FP32-mixed against plain FP64 on the 32^4 configuration: generator G
+    seed 11, eps 0.01 to t=5.0 (500 steps), E/Q every 10 steps, FP32 links
+    reunitarised every 10 steps."""
+    import numpy as np
+    from msc_project_b200 import FP32MIXED, FP64
+    shape, steps, meas = (32, 32, 32, 32), 500, 10
+    V = int(np.prod(shape))
+    res = {}
+    for name, prec, reunit in (("fp64", FP64, 0), ("fp32mixed", FP32MIXED, 10)):
+        with ctx.lattice(shape, prec) as lat:
+            lat.generate(11, 0.5)
+            _flow_timed(ctx, lat, 0.01, 20, 10, reunit)  # warm-up: module load, graph capture
+            lat.generate(11, 0.5)
+            r, sec = _flow_timed(ctx, lat, 0.01, steps, meas, reunit)
+            u, d = lat.unitarity()
+        res[name] = (r, sec, u, d)
+    r64, s64, _, _ = res["fp64"]
+    r32, s32, u32, d32 = res["fp32mixed"]
+    return {"config": "32^4 G seed 11, eps 0.01, 500 steps, E/Q every 10, reunitarise every 10",
+            "fp64_site_steps_per_s": V * steps / s64, "fp32mixed_site_steps_per_s": V * steps / s32,
+            "speedup": s64 / s32,
+            "max_rel_dE": float(np.max(np.abs(r32.E - r64.E) / np.abs(r64.E))),
+            "max_abs_dQ": float(np.max(np.abs(r32.Q - r64.Q))),
+            "max_unit_err": u32, "max_det_err": d32,
+            "gates": {"dQ<1e-3": bool(np.max(np.abs(r32.Q - r64.Q)) < 1e-3),
+                      "dE/E<1e-5": bool(np.max(np.abs(r32.E - r64.E) / np.abs(r64.E)) < 1e-5)}}
+
+
+ENSEMBLE = [((8, 8, 8, 8), 16), ((12, 12, 12, 12), 16), ((16, 16, 16, 16), 16), ((32, 16, 16, 16), 8),
+            ((48, 24, 24, 24), 8)]
+
+
+def form_batched(ctx):
+    """The 64-configuration ensemble of uneven volumes (seeds 100-163), eps 0.01
+    to t=2.0 (200 steps), E/Q every 10 steps: one batched run per precision
+    against the same jobs flowed one after another with lgf_flow."""
+    import numpy as np
+    from msc_project_b200 import FP32MIXED, FP64, Job
+    out = {}
+    results = {}
+    for name, prec, reunit in (("fp64", FP64, 0), ("fp32mixed", FP32MIXED, 10)):
+        def jobs():
+            js, seed = [], 100
+            for shape, n in ENSEMBLE:
+                for _ in range(n):
+                    js.append(Job(shape, prec, seed=seed, nsteps=200, meas_every=10, reunit_every=reunit))
+                    seed += 1
+            return js
+        ctx.batch_run([Job((8, 8, 8, 8), prec, seed=1, nsteps=10, meas_every=10, reunit_every=reunit)])  # warm-up
+        js = jobs()
+        st = ctx.batch_run(js)
+        seq = 0.0
+        for j in jobs():
+            with ctx.lattice(j.shape, prec) as lat:
+                lat.generate(j.seed, 0.5)
+                _, sec = _flow_timed(ctx, lat, 0.01, 200, 10, reunit)
+                seq += sec
+        out[name] = {"site_steps_per_s": st.site_steps / st.seconds, "seconds": st.seconds,
+                     "sequential_seconds": seq, "batching_speedup": seq / st.seconds,
+                     "launches": st.launches, "block_threads": st.block_threads}
+        results[name] = js
+    dq = max(float(np.max(np.abs(a.result.Q - b.result.Q))) for a, b in zip(results["fp32mixed"], results["fp64"]))
+    de = max(float(np.max(np.abs(a.result.E - b.result.E) / np.abs(b.result.E)))
+             for a, b in zip(results["fp32mixed"], results["fp64"]))
+    out["configs"] = 64
+    out["sites"] = int(sum(np.prod(s) * n for s, n in ENSEMBLE))
+    out["fp32mixed_vs_fp64"] = {"max_abs_dQ": dq, "max_rel_dE": de,
+                                "speedup": out["fp32mixed"]["site_steps_per_s"] / out["fp64"]["site_steps_per_s"]}
+    return out
+
+
+def form_served(ctx, njobs: int, rate: float, seed: int = 5):
+    """A served stream: Poisson arrivals (rate jobs/s) of FP32-mixed jobs with
+    volume uniform over {16^4, 24^3x48, 32^4, 48^4}, t_max ~ U[1,8], eps 0.01,
+    E/Q every 5 steps, per-job seed; admission by HBM footprint."""
+    import numpy as np
+    from msc_project_b200 import FP32MIXED, Job, Server
+    rng = np.random.default_rng(seed)
+    vols = [(16, 16, 16, 16), (48, 24, 24, 24), (32, 32, 32, 32), (48, 48, 48, 48)]
+    jobs = []
+    for i in range(njobs):
+        shape = vols[int(rng.integers(0, 4))]
+        tmax = float(rng.uniform(1.0, 8.0))
+        jobs.append(Job(shape, FP32MIXED, seed=1000 + i, nsteps=int(round(tmax / 0.01)), meas_every=5,
+                        reunit_every=10))
+    gaps = rng.exponential(1.0 / rate, size=njobs)
+    try:
+        import torch
+        free, _ = torch.cuda.mem_get_info()
+    except Exception:
+        free = 120 << 30
+    budget = int(free * 0.6)
+    with Server(ctx, budget, max_active=16, steps_per_tick=5) as srv:
+        srv.submit(Job((16, 16, 16, 16), FP32MIXED, seed=1, nsteps=5, meas_every=5, reunit_every=10))  # warm-up
+        ids = []
+        t0 = time.perf_counter()
+        for j, g in zip(jobs, gaps):
+            time.sleep(float(g))
+            ids.append(srv.submit(j))
+        sts = [srv.wait(i, 3600.0) for i in ids]
+        makespan = time.perf_counter() - t0
+    lat = np.array([s.end_s - s.submit_s for s in sts])
+    work = sum(int(np.prod(j.shape)) * j.nsteps for j in jobs)
+    return {"jobs": njobs, "rate_per_s": rate, "jobs_per_s": njobs / makespan,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "site_steps_per_s": work / makespan, "hbm_budget_bytes": budget,
+            "all_done": all(s.state == 2 for s in sts)}
+
+
 # ------------------------------------------------------------------ engine
 def engine_arm(args):
     import numpy as np
@@ -272,6 +390,11 @@ def engine_arm(args):
         else:
             cpu = {"value": None, "unavailable": err}
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = {"fp32mixed": form_fp32mixed(ctx), "batched": form_batched(ctx),
+                 "served": form_served(ctx, args.serve_jobs, args.serve_rate)}
+
     launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
     line = {
         "metric": "site-RK3-steps/s", "value": value, "unit": "site-RK3-steps/s", "n_gpus": world,
@@ -289,6 +412,7 @@ def engine_arm(args):
         "fp64_pipe": {"achieved_tflops": stage_tflops, "nominal_peak_tflops_at_clock": fma_peak,
                       "frac": stage_tflops / fma_peak, "note": "canonical flops / stage time vs 148 SM x 64 FP64 FMA x 2 x median SM clock"},
         "cpu_baseline": cpu,
+        "forms": forms,
         "clocks": clocks,
         "gpu_launches": launches_per_job * args.steps,
         "wall_s": wall,
@@ -301,6 +425,21 @@ def engine_arm(args):
         dist.destroy_process_group()
 
 
+def profile_case(args):
+    """One launch of each RK3 stage kernel and of the measurement kernel on the
+    bench lattice (the case the ncu captures under profiles/ use)."""
+    import numpy as np
+    from msc_project_b200 import FP32MIXED, FP64, Context
+    prec = FP64 if args.precision == "fp64" else FP32MIXED
+    with Context(0) as ctx, ctx.lattice(SHAPE, prec) as lat:
+        lat.generate(SEED, 0.5)
+        ms = (ctypes.c_double * 4)()
+        ctx.check(ctx.lib.lgf_profile_kernels(lat.h, EPS, 1, ms))  # first launches load the modules
+        ctx.check(ctx.lib.lgf_profile_kernels(lat.h, EPS, args.profile_reps, ms))
+        print(json.dumps({"profile_case": list(SHAPE), "precision": args.precision,
+                          "stage_ms": [ms[0], ms[1], ms[2]], "measure_ms": ms[3]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -310,8 +449,15 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "fp32mixed"], default="fp64")
     ap.add_argument("--ref-procs", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, batched and served forms")
+    ap.add_argument("--serve-jobs", type=int, default=12)
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson arrival rate, jobs/s")
+    ap.add_argument("--profile", action="store_true", help="one launch of each kernel (for ncu captures)")
+    ap.add_argument("--profile-reps", type=int, default=1)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile:
+        profile_case(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         engine_arm(args)

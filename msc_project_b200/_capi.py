@@ -102,12 +102,14 @@ _lib = None
 
 
 def load(path: Path | None = None) -> ctypes.CDLL:
-    """Load liblgf_b200.so (built in-tree by msc_project_b200.build).  Raises
-    if it is missing or lacks a declared symbol."""
+    """Load liblgf_b200.so (built in-tree by msc_project_b200.build, or the
+    file named by $LGF_LIB).  Raises if it is missing or lacks a declared
+    symbol."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    import os
+    p = Path(path) if path else Path(os.environ.get("LGF_LIB", LIB_PATH))
     if not p.exists():
         raise RuntimeError(f"{p} is missing: build it with `python -m msc_project_b200.build` "
                            "(the engine has no CPU fallback)")

@@ -163,7 +163,7 @@ int tune_threads(lgf_ctx* ctx, int prec, const int shape_in[4], int* best) {
     if (rc != LGF_OK) return rc;
     rc = launch_generate(ctx, b, 12345, 0.5);
     b.eps = 0.01;
-    const int cands[] = {64, 128, 256};
+    const int cands[] = {128, 256};  // multiples of 128: a tile holds all four directions of 32-site groups
     float best_ms = 1e30f;
     int best_t = default_threads(prec);
     cudaEvent_t e0, e1;

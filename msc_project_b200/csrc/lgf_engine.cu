@@ -171,8 +171,8 @@ public:
             d.slot = b.slot;
             d.nchunk = b.nchunk;
             d.eps = (R)b.eps;
-            const long long nl = 4LL * b.g.V;
-            for (long long t0 = 0; t0 < nl; t0 += threads_) tiles.push_back(make_int2((int)i, (int)t0));
+            // a tile is threads_/4 consecutive sites with all four link directions
+            for (long long s0 = 0; s0 < b.g.V; s0 += threads_ / 4) tiles.push_back(make_int2((int)i, (int)s0));
             mt += (long long)b.g.n[0] * b.nchunk;
         }
         if ((long long)tiles.size() > max_tiles_)

@@ -24,6 +24,18 @@
 #pragma once
 #include "lgf_lattice.cuh"
 
+// Launch bounds of the two hot kernels: (max threads per block, min resident
+// blocks per SM).  The second number caps the registers per thread.
+#ifndef LGF_STAGE_MAXT
+#define LGF_STAGE_MAXT 256
+#endif
+#ifndef LGF_STAGE_MINB
+#define LGF_STAGE_MINB 1
+#endif
+#ifndef LGF_MEAS_MINB
+#define LGF_MEAS_MINB 2  // 2 blocks of 192 per SM: measured faster than 1 block without a register cap
+#endif
+
 namespace lgf {
 
 // ----------------------------------------------------------------- staple
@@ -34,15 +46,16 @@ template <typename R>
 __device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                 int mu, su3<R>& u_out) {
     const int V = g.V;
+    const Dir dm = dir_of(g, c, mu);
     su3<R> S;
     su3_zero(S);
-    const int xpm = fwd(g, s, mu, c.x[mu]);
+    const int xpm = fwd(s, dm);
 #pragma unroll
     for (int nu = 0; nu < 4; ++nu) {
         if (nu == mu) continue;
         const int xpn = fwd(g, s, nu, c.x[nu]);
         const int xmn = bwd(g, s, nu, c.x[nu]);
-        const int xmnpm = fwd(g, xmn, mu, c.x[mu]);
+        const int xmnpm = fwd(xmn, dm);  // the mu coordinate of x-nu is x_mu
         {
             su3<R> a2 = load_link(U, V, nu, s);
             su3<R> a3 = load_link(U, V, mu, xpn);
@@ -86,24 +99,26 @@ template <typename R> struct LatDesc {
 //   S=3:                             U3 = exp(eps (3/4 Z2 - A)) U2
 // which equals GradientFlow.cpp:27-50 term by term.  Input and output are
 // different buffers of the ring (every thread reads neighbours of the input).
-// Persistent: blocks stride over the tile list; tile = (lattice, first link
-// thread); link thread t -> (mu = t / V, s = t % V).
+// Persistent: blocks stride over the tile list; tile = (lattice, first site).
+// A tile of T threads (T a multiple of 128) covers T/4 consecutive sites with
+// all four directions: warp w handles mu = w % 4 for the 32 sites of group
+// w / 4, so the four link directions of a site range are read together and
+// every load of a warp covers 32 consecutive sites.
 template <typename R, int S>
-__global__ void __launch_bounds__(256) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
+__global__ void __launch_bounds__(LGF_STAGE_MAXT, LGF_STAGE_MINB) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
                                                    const int* __restrict__ ntiles) {
     const int n = *ntiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
         const int2 tile = tiles[ti];
         const LatDesc<R>* d = descs + tile.x;
         const Geom g = d->g;
-        const int t = tile.y + threadIdx.x;
-        if (t >= 4 * g.V) continue;
+        const int mu = (threadIdx.x >> 5) & 3;
+        const int s = tile.y + ((threadIdx.x >> 7) << 5) + (threadIdx.x & 31);
+        if (s >= g.V) continue;
         const cplx<R>* Uin = S == 1 ? d->U0 : (S == 2 ? d->U1 : d->U2);
         cplx<R>* Uout = S == 1 ? d->U1 : (S == 2 ? d->U2 : d->U0);
         R* A = d->A;
         const R eps = d->eps;
-        const int mu = t / g.V;
-        const int s = t - mu * g.V;
         const Coord c = site_coord(g, s);
         su3<R> u;
         const alg<R> Z = flow_gradient<R>(Uin, g, s, c, mu, u);
@@ -127,99 +142,193 @@ __global__ void __launch_bounds__(256) k_rk3_stage(const LatDesc<R>* __restrict_
 }
 
 // ---------------------------------------------------------- Wilson loops
-// Walks a closed a x b rectangle starting at x in the plane (mu, nu): a step
-// +d multiplies U_d(y) and moves y -> y+d, a step -d moves y -> y-d and
-// multiplies U_d(y)^dag.  Quadrant q selects the leaf, in the orientation the
-// reference uses for all its clover-type averages (SU3_field.cpp:550-560,
-// 606-631, 654-694, 723-775):
+// The clover-type averages of the reference (SU3_field.cpp:533-792) are sums
+// of a x b rectangular loops through x, one per quadrant, in the orientation
 //   q0: +nu^b +mu^a -nu^b -mu^a     q1: +mu^a -nu^b -mu^a +nu^b
 //   q2: -mu^a +nu^b +mu^a -nu^b     q3: -nu^b -mu^a +nu^b +mu^a
-template <typename R> struct Walker {
-    const cplx<R>* __restrict__ U;
-    Geom g;
-    int y, ymu, ynu, mu, nu;
-    su3<R> acc;
-    bool first;
+// (a links along mu, b along nu).  With quadrant signs (sm, sn) = (+,+),
+// (+,-), (-,+), (-,-), every leaf is  Pn Pm^dag  (q0, q3) or its adjoint
+// (q1, q2), where Pn = (sn nu)^b (sm mu)^a and Pm = (sm mu)^a (sn nu)^b are
+// the two L-shaped paths from x to the far corner.  The projection F[W] is
+// linear and F[W^dag] = -F[W], so each quadrant adds sign * F[Pn Pm^dag]
+// with sign = +1 for q0, q3 and -1 for q1, q2, weighted per shape:
+//   F^ = 19/9 F[C11] + 1/36 F[C22] - 32/45 F[C12] + 1/15 F[C13]
+//      C11 = 1/4 (1x1), C22 = 1/4 (2x2), C12 = 1/8 (1x2 + 2x1), C13 = 1/8 (1x3 + 3x1)
+// (SU3_field.cpp:588-597), and the clover F = F[C11] for E.  The paths are
+// built as shared chains (a path of a shape extends the path of the shape
+// before it by one link), 27 matrix products and 27 link loads per quadrant
+// instead of 34 and 40 for separate loops.
+struct PlanePos { int s, xm, xn; };
 
-    __device__ __forceinline__ void step(int dir, int sign) {
-        int& yc = (dir == mu) ? ymu : ynu;
-        su3<R> l;
+template <typename R> struct Plane {
+    const cplx<R>* __restrict__ U;
+    int V, mu, nu;
+    Dir dm, dn;  // .x unused: positions carry their own coordinates
+
+    // the link of one step from p and the new position; adjoint for a backward step
+    __device__ __forceinline__ su3<R> step(PlanePos& p, bool along_mu, int sign) const {
+        const Dir& d = along_mu ? dm : dn;
+        int& xc = along_mu ? p.xm : p.xn;
+        const int dir = along_mu ? mu : nu;
         if (sign > 0) {
-            l = load_link(U, g.V, dir, y);
-            y = fwd(g, y, dir, yc);
-            yc = wrap_inc(yc, g.n[dir]);
-            if (first) acc = l;
-            else acc = mul_nn(acc, l);
-        } else {
-            y = bwd(g, y, dir, yc);
-            yc = wrap_dec(yc, g.n[dir]);
-            l = load_link(U, g.V, dir, y);
-            if (first) {
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int cc = 0; cc < 3; ++cc)
-                        acc.m[3 * r + cc] = cmk<R>(l.m[3 * cc + r].re, -l.m[3 * cc + r].im);
-            } else {
-                acc = mul_na(acc, l);
-            }
+            su3<R> l = load_link(U, V, dir, p.s);
+            p.s = (xc == d.n - 1) ? p.s - (d.n - 1) * d.stride : p.s + d.stride;
+            xc = wrap_inc(xc, d.n);
+            return l;
         }
-        first = false;
+        p.s = (xc == 0) ? p.s + (d.n - 1) * d.stride : p.s - d.stride;
+        xc = wrap_dec(xc, d.n);
+        su3<R> l = load_link(U, V, dir, p.s);
+        su3<R> a;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) a.m[3 * r + c] = cmk<R>(l.m[3 * c + r].re, -l.m[3 * c + r].im);
+        return a;
     }
-    __device__ __forceinline__ void seg(int dir, int sign, int len) {
-        for (int i = 0; i < len; ++i) step(dir, sign);
+    // P <- P * (link of one step from p)
+    __device__ __forceinline__ void ext(su3<R>& P, PlanePos& p, bool along_mu, int sign) const {
+        const Dir& d = along_mu ? dm : dn;
+        int& xc = along_mu ? p.xm : p.xn;
+        const int dir = along_mu ? mu : nu;
+        if (sign > 0) {
+            const su3<R> l = load_link(U, V, dir, p.s);
+            p.s = (xc == d.n - 1) ? p.s - (d.n - 1) * d.stride : p.s + d.stride;
+            xc = wrap_inc(xc, d.n);
+            P = mul_nn(P, l);
+        } else {
+            p.s = (xc == 0) ? p.s + (d.n - 1) * d.stride : p.s - d.stride;
+            xc = wrap_dec(xc, d.n);
+            const su3<R> l = load_link(U, V, dir, p.s);
+            P = mul_na(P, l);
+        }
     }
 };
 
-template <typename R, int A, int B>
-__device__ __forceinline__ void add_leaves(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c, int mu,
-                                           int nu, su3<R>& sum) {
-#pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
-        Walker<R> w;
-        w.U = U;
-        w.g = g;
-        w.y = s;
-        w.ymu = c.x[mu];
-        w.ynu = c.x[nu];
-        w.mu = mu;
-        w.nu = nu;
-        w.first = true;
-        if (q == 0) { w.seg(nu, +1, B); w.seg(mu, +1, A); w.seg(nu, -1, B); w.seg(mu, -1, A); }
-        else if (q == 1) { w.seg(mu, +1, A); w.seg(nu, -1, B); w.seg(mu, -1, A); w.seg(nu, +1, B); }
-        else if (q == 2) { w.seg(mu, -1, A); w.seg(nu, +1, B); w.seg(mu, +1, A); w.seg(nu, -1, B); }
-        else { w.seg(nu, -1, B); w.seg(mu, -1, A); w.seg(nu, +1, B); w.seg(mu, +1, A); }
-        su3_addto(sum, w.acc);
+// F += c * F[A B^dag] without forming the product: only the entries the
+// projection reads (Im of the diagonal, both triangles) are computed.
+template <typename R> __device__ __forceinline__ void leaf_acc(const su3<R>& A, const su3<R>& B, R c, alg<R>& F) {
+    // W_ij = sum_k A_ik conj(B_jk)
+    R d[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R im = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) im = fma(A.m[3 * i + k].im, B.m[3 * i + k].re, fma(-A.m[3 * i + k].re, B.m[3 * i + k].im, im));
+        d[i] = im;
+    }
+    const R tr = (d[0] + d[1] + d[2]) * R(1.0 / 3.0);
+    F.v[0] = fma(c, d[0] - tr, F.v[0]);
+    F.v[1] = fma(c, d[1] - tr, F.v[1]);
+    const int I[3] = {0, 0, 1}, J[3] = {1, 2, 2};
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        const int i = I[o], j = J[o];
+        cplx<R> wij = cmulc(A.m[3 * i], B.m[3 * j]);
+        wij = cfmac(A.m[3 * i + 1], B.m[3 * j + 1], wij);
+        wij = cfmac(A.m[3 * i + 2], B.m[3 * j + 2], wij);
+        cplx<R> wji = cmulc(A.m[3 * j], B.m[3 * i]);
+        wji = cfmac(A.m[3 * j + 1], B.m[3 * i + 1], wji);
+        wji = cfmac(A.m[3 * j + 2], B.m[3 * i + 2], wji);
+        // (-i/2)(a + ib) = (b/2, -a/2),  a + ib = W_ij - conj(W_ji)
+        const R a = wij.re - wji.re, b = wij.im + wji.im;
+        F.v[2 + 2 * o] = fma(R(0.5) * c, b, F.v[2 + 2 * o]);
+        F.v[3 + 2 * o] = fma(R(-0.5) * c, a, F.v[3 + 2 * o]);
     }
 }
 
-// Clover F and improved F for plane (mu, nu) at site s:
-//   F   = F[C11],  C11 = 1/4 (1x1 leaves)
-//   F^  = 19/9 F[C11] + 1/36 F[C22] - 32/45 F[C12] + 1/15 F[C13]
-// with C22 = 1/4 (2x2), C12 = 1/8 (1x2 + 2x1), C13 = 1/8 (1x3 + 3x1)
-// (SU3_field.cpp:588-597).
 template <typename R>
 __device__ __forceinline__ void plane_fields(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                              int mu, int nu, alg<R>& F11, alg<R>& Fhat) {
-    su3<R> C;
-    su3_zero(C);
-    add_leaves<R, 1, 1>(U, g, s, c, mu, nu, C);
-    F11 = field_strength(C, R(0.25));
-    Fhat = alg_scale(R(19.0 / 9.0), F11);
-    su3_zero(C);
-    add_leaves<R, 2, 2>(U, g, s, c, mu, nu, C);
-    alg<R> f = field_strength(C, R(0.25));
-    Fhat = alg_axpby(R(1), Fhat, R(1.0 / 36.0), f);
-    su3_zero(C);
-    add_leaves<R, 1, 2>(U, g, s, c, mu, nu, C);
-    add_leaves<R, 2, 1>(U, g, s, c, mu, nu, C);
-    f = field_strength(C, R(1.0 / 8.0));
-    Fhat = alg_axpby(R(1), Fhat, R(-32.0 / 45.0), f);
-    su3_zero(C);
-    add_leaves<R, 1, 3>(U, g, s, c, mu, nu, C);
-    add_leaves<R, 3, 1>(U, g, s, c, mu, nu, C);
-    f = field_strength(C, R(1.0 / 8.0));
-    Fhat = alg_axpby(R(1), Fhat, R(1.0 / 15.0), f);
+    Plane<R> P;
+    P.U = U;
+    P.V = g.V;
+    P.mu = mu;
+    P.nu = nu;
+    P.dm = dir_of(g, c, mu);
+    P.dn = dir_of(g, c, nu);
+    const PlanePos x0 = {s, P.dm.x, P.dn.x};
+    const R k11 = R(19.0 / 36.0), k12 = R(-4.0 / 45.0), k13 = R(1.0 / 120.0), k22 = R(1.0 / 144.0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        F11.v[k] = R(0);
+        Fhat.v[k] = R(0);
+    }
+    alg<R> G;  // 1x1 leaves, for both F and F^
+#pragma unroll
+    for (int k = 0; k < 8; ++k) G.v[k] = R(0);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        const int sm = (q == 0 || q == 1) ? 1 : -1;
+        const int sn = (q == 0 || q == 2) ? 1 : -1;
+        const R sg = (q == 0 || q == 3) ? R(1) : R(-1);
+        // row: shapes (1,1), (2,1), (3,1)
+        PlanePos pn = x0, pm = x0;
+        su3<R> Rn = P.step(pn, false, sn);  // (sn nu)
+        su3<R> Lm = P.step(pm, true, sm);   // (sm mu)
+        P.ext(Rn, pn, true, sm);            // Pn(1,1)
+        {
+            PlanePos q2 = pm;
+            su3<R> Pm = Lm;
+            P.ext(Pm, q2, false, sn);        // Pm(1,1)
+            leaf_acc(Rn, Pm, sg, G);
+        }
+        P.ext(Rn, pn, true, sm);            // Pn(2,1)
+        P.ext(Lm, pm, true, sm);            // (sm mu)^2
+        {
+            PlanePos q2 = pm;
+            su3<R> Pm = Lm;
+            P.ext(Pm, q2, false, sn);        // Pm(2,1)
+            leaf_acc(Rn, Pm, sg * k12, Fhat);
+        }
+        P.ext(Rn, pn, true, sm);            // Pn(3,1)
+        P.ext(Lm, pm, true, sm);            // (sm mu)^3
+        {
+            PlanePos q2 = pm;
+            su3<R> Pm = Lm;
+            P.ext(Pm, q2, false, sn);        // Pm(3,1)
+            leaf_acc(Rn, Pm, sg * k13, Fhat);
+        }
+        // column: shapes (1,2), (1,3)
+        pn = x0;
+        Rn = P.step(pn, false, sn);
+        P.ext(Rn, pn, false, sn);           // (sn nu)^2
+        pm = x0;
+        Lm = P.step(pm, true, sm);
+        P.ext(Lm, pm, false, sn);
+        P.ext(Lm, pm, false, sn);           // Pm(1,2)
+        {
+            PlanePos q2 = pn;
+            su3<R> Pn = Rn;
+            P.ext(Pn, q2, true, sm);         // Pn(1,2)
+            leaf_acc(Pn, Lm, sg * k12, Fhat);
+        }
+        P.ext(Rn, pn, false, sn);           // (sn nu)^3
+        P.ext(Lm, pm, false, sn);           // Pm(1,3)
+        {
+            PlanePos q2 = pn;
+            su3<R> Pn = Rn;
+            P.ext(Pn, q2, true, sm);         // Pn(1,3)
+            leaf_acc(Pn, Lm, sg * k13, Fhat);
+        }
+        // (2,2)
+        pn = x0;
+        Rn = P.step(pn, false, sn);
+        P.ext(Rn, pn, false, sn);
+        P.ext(Rn, pn, true, sm);
+        P.ext(Rn, pn, true, sm);            // Pn(2,2)
+        pm = x0;
+        Lm = P.step(pm, true, sm);
+        P.ext(Lm, pm, true, sm);
+        P.ext(Lm, pm, false, sn);
+        P.ext(Lm, pm, false, sn);           // Pm(2,2)
+        leaf_acc(Rn, Lm, sg * k22, Fhat);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        F11.v[k] = R(0.25) * G.v[k];
+        Fhat.v[k] = fma(k11, G.v[k], Fhat.v[k]);
+    }
 }
 
 __device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
@@ -236,7 +345,7 @@ constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
 //        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
 //                                             (TopologicalCharge.cpp:11-16)
 template <typename R>
-__global__ void __launch_bounds__(MEAS_SITES * 6) k_measure(const LatDesc<R>* __restrict__ descs,
+__global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const LatDesc<R>* __restrict__ descs,
                                                             const int4* __restrict__ mtiles,
                                                             const int* __restrict__ nmtiles,
                                                             double* __restrict__ site_e, double* __restrict__ site_q) {

@@ -58,6 +58,24 @@ __device__ __forceinline__ int bwd(const Geom& g, int s, int d, int xd) {
 __device__ __forceinline__ int wrap_inc(int x, int n) { return x == n - 1 ? 0 : x + 1; }
 __device__ __forceinline__ int wrap_dec(int x, int n) { return x == 0 ? n - 1 : x - 1; }
 
+// One lattice direction as plain scalars (extent, stride, and the thread's
+// coordinate along it).  Selected without indexing a local array, so nothing
+// spills to local memory when the direction is only known at run time.
+struct Dir { int n, stride, x; };
+
+__device__ __forceinline__ int sel4(int d, int a0, int a1, int a2, int a3) {
+    return d == 0 ? a0 : (d == 1 ? a1 : (d == 2 ? a2 : a3));
+}
+__device__ __forceinline__ Dir dir_of(const Geom& g, const Coord& c, int d) {
+    Dir r;
+    r.n = sel4(d, g.n[0], g.n[1], g.n[2], g.n[3]);
+    r.stride = sel4(d, g.stride[0], g.stride[1], g.stride[2], g.stride[3]);
+    r.x = sel4(d, c.x[0], c.x[1], c.x[2], c.x[3]);
+    return r;
+}
+__device__ __forceinline__ int fwd(int s, const Dir& d) { return (d.x == d.n - 1) ? s - (d.n - 1) * d.stride : s + d.stride; }
+__device__ __forceinline__ int bwd(int s, const Dir& d) { return (d.x == 0) ? s + (d.n - 1) * d.stride : s - d.stride; }
+
 template <typename R> struct vec2_of;
 template <> struct vec2_of<double> { typedef double2 type; };
 template <> struct vec2_of<float> { typedef float2 type; };
