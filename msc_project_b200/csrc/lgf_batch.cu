@@ -1,11 +1,16 @@
 // Batched flow of many configurations of uneven volumes, and the autotuner.
 //
-// All jobs of one precision are members of one group: every RK3 stage of
-// every job is a single persistent launch over the group's shared tile list,
-// one RK3 step (three stage launches) is captured once as a CUDA graph and
-// replayed, and jobs that finish early leave the work list (the graph reads
-// the list and its length from device memory, so it is not re-captured).
-// Each job's arithmetic is exactly what lgf_flow does for it alone.
+// Jobs of one precision are packed, smallest first, into waves whose working
+// set of one RK3 stage (input and output link buffers plus the su(3)
+// accumulator) fits in the 126 MB L2 (budget 96 MB).  A wave is one group:
+// every RK3 stage of all its jobs is a single persistent launch over the
+// wave's shared tile list, one RK3 step (three stage launches) is captured
+// once as a CUDA graph and replayed, and jobs that finish early leave the
+// work list (the graph reads the list and its length from device memory, so
+// it is not re-captured).  Waves run one after another, so a wave's links stay
+// in L2 from one stage to the next; a job too large for any wave forms a wave
+// of its own (it fills the GPU alone).  Each job's arithmetic is exactly what
+// lgf_flow does for it alone.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -154,6 +159,29 @@ int run_group(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, int threads, i
     return LGF_OK;
 }
 
+// L2-sized waves: jobs sorted by volume, packed greedily while the wave's
+// per-stage working set fits the budget; order inside a wave is the input order.
+const size_t L2_WAVE_BYTES = 96u << 20;
+
+std::vector<std::vector<JobRun*>> l2_waves(const std::vector<JobRun*>& jobs, int prec) {
+    const size_t rs = prec == LGF_PREC_FP64 ? 8 : 4;
+    auto stage_bytes = [&](const JobRun* r) { return (size_t)r->buf.g.V * 4 * (2 * 18 + 8) * rs; };
+    std::vector<JobRun*> order = jobs;
+    std::stable_sort(order.begin(), order.end(), [](const JobRun* a, const JobRun* b) { return a->buf.g.V < b->buf.g.V; });
+    std::vector<std::vector<JobRun*>> waves;
+    size_t cur = 0;
+    for (JobRun* r : order) {
+        const size_t b = stage_bytes(r);
+        if (waves.empty() || cur + b > L2_WAVE_BYTES) {
+            waves.emplace_back();
+            cur = 0;
+        }
+        waves.back().push_back(r);
+        cur += b;
+    }
+    return waves;
+}
+
 int tune_threads(lgf_ctx* ctx, int prec, const int shape_in[4], int* best) {
     // a lattice of the job's shape, capped so tuning stays well under a second
     int shape[4] = {shape_in[0], shape_in[1], shape_in[2], shape_in[3]};
@@ -269,7 +297,10 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
     for (int prec = 0; prec < 2 && rc == LGF_OK; ++prec) {
         if (groups[prec].empty()) continue;
         threads_used = threads[prec];
-        rc = run_group(ctx, prec, groups[prec], threads[prec], &launches);
+        for (auto& wave : l2_waves(groups[prec], prec)) {
+            rc = run_group(ctx, prec, wave, threads[prec], &launches);
+            if (rc != LGF_OK) break;
+        }
     }
     cudaEventRecord(e1, ctx->stream);
     cudaError_t e = cudaEventSynchronize(e1);
