@@ -52,7 +52,7 @@ BYTES_PER_SITE_STAGE = {0: 4480.0 / 3, 1: 2240.0 / 3}
 FLOPS_PER_SITE_STAGE = 42888.0 / 3
 # DRAM traffic of one stage launch from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum), scaled to this workload; see profiles/.
-NCU_STAGE_TRAFFIC_BYTES = None
+NCU_STAGE_TRAFFIC_BYTES = {0: 1156.2e6, 1: 527.8e6}  # stage-2 launch; profiles/k_rk3_stage_*_24x24x24x48.md
 FP64_FMA_PER_SM_PER_CLK = 64  # B200: 64 FP64 FMA lanes per SM (nominal)
 N_SM = 148
 
@@ -422,7 +422,7 @@ def engine_arm(args):
                 "d2h_bytes_per_step": nmeas * 3 * 8},
         "roofline": {"bound": "hbm", "kernel": "k_rk3_stage (mean of the 3 stages)", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": NCU_STAGE_TRAFFIC_BYTES, "stage_ms": stage_ms, "measure_ms": ms[3]},
+                     "traffic": NCU_STAGE_TRAFFIC_BYTES[prec], "traffic_note": "DRAM bytes of one stage-2 launch (ncu), algorithmic 1104 MB (FP64) / 552 MB (FP32)", "stage_ms": stage_ms, "measure_ms": ms[3]},
         "fp64_pipe": {"achieved_tflops": stage_tflops, "nominal_peak_tflops_at_clock": fma_peak,
                       "frac": stage_tflops / fma_peak, "note": "canonical flops / stage time vs 148 SM x 64 FP64 FMA x 2 x median SM clock"},
         "cpu_baseline": cpu,

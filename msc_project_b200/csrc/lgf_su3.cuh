@@ -188,7 +188,8 @@ template <typename R> __device__ __forceinline__ herm_d herm_from_alg(const alg<
 }
 
 // Cayley-Hamilton coefficients f0, f1, f2 with exp(iQ) = f0 + f1 Q + f2 Q^2
-// for Hermitian traceless Q (Morningstar & Peardon, hep-lat/0311018, eqs.
+// for Hermitian traceless Q.  Below c1 = 0.25 the series form above; from
+// there the closed form of Morningstar & Peardon (hep-lat/0311018, eqs.
 // 14-34), with the reference's branch structure and thresholds
 // (LGF/Math/SU3_mat.cpp:216-289): analytic form when c1 > 1e-4, otherwise the
 // two-variable series; xi0 = sin(w)/w by series when |w| <= 0.05; the
@@ -196,8 +197,42 @@ template <typename R> __device__ __forceinline__ herm_d herm_from_alg(const alg<
 // c1 = ReTr(Q^2)/2 are taken as inputs.  The acos argument is clamped to
 // [0, 1] (the reference clamps only in its _DEBUG build, SU3_mat.cpp:231-238;
 // without the clamp a rounding excess above 1 would give NaN).
+// Series form used below c1 = 0.25 (eigenvalues |lambda| <= 2 sqrt(c1/3) < 0.58):
+// with Q^3 = c1 Q + c0 (Cayley-Hamilton), Q^n = a_n + b_n Q + d_n Q^2 where
+// a_{n+1} = c0 d_n, b_{n+1} = a_n + c1 d_n, d_{n+1} = b_n, and
+// f_j = sum_n i^n {a,b,d}_n / n!.  17 terms leave a remainder below 1e-19, so
+// it agrees with the closed form to rounding while needing no transcendental
+// function (the flow's exponents are small: c1 is ~1e-5..1e-2 at eps = 0.01).
+__device__ __forceinline__ void ch_series(double c0, double c1, cplx<double>& f0, cplx<double>& f1,
+                                          cplx<double>& f2) {
+    double a = 1.0, b = 0.0, d = 0.0, inv = 1.0;
+    double r0 = 1.0, i0 = 0.0, r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
+#pragma unroll
+    for (int n = 1; n <= 17; ++n) {
+        const double an = c0 * d, bn = fma(c1, d, a);
+        d = b;
+        a = an;
+        b = bn;
+        inv *= 1.0 / (double)n;
+        const double ta = a * inv, tb = b * inv, td = d * inv;
+        switch (n & 3) {  // i^n
+            case 0: r0 += ta; r1 += tb; r2 += td; break;
+            case 1: i0 += ta; i1 += tb; i2 += td; break;
+            case 2: r0 -= ta; r1 -= tb; r2 -= td; break;
+            default: i0 -= ta; i1 -= tb; i2 -= td; break;
+        }
+    }
+    f0 = cmk<double>(r0, i0);
+    f1 = cmk<double>(r1, i1);
+    f2 = cmk<double>(r2, i2);
+}
+
 __device__ __forceinline__ void ch_coefficients(double c0, double c1, cplx<double>& f0, cplx<double>& f1,
                                                 cplx<double>& f2) {
+    if (c1 < 0.25) {
+        ch_series(c0, c1, f0, f1, f2);
+        return;
+    }
     if (c1 > 0.0001) {
         const double c1s = sqrt(c1);
         const double t = c1 * (1.0 / 3.0);

@@ -36,6 +36,26 @@ def test_exp_against_reference(ctx):
     assert np.max(np.abs(out32 - z["exp"])) < 5e-6
 
 
+def test_exp_against_expm_over_all_scales(ctx):
+    """The series (c1 < 0.25) and closed-form (c1 >= 0.25) coefficient paths
+    both agree with a dense matrix exponential to rounding."""
+    import scipy.linalg as sl
+    rng = np.random.default_rng(11)
+    n = 400
+    H = rng.normal(size=(n, 3, 3)) + 1j * rng.normal(size=(n, 3, 3))
+    H = (H + np.conj(np.transpose(H, (0, 2, 1)))) / 2
+    H -= np.trace(H, axis1=1, axis2=2)[:, None, None] / 3 * np.eye(3)
+    H /= np.linalg.norm(H, axis=(1, 2))[:, None, None]
+    scale = np.exp(rng.uniform(np.log(1e-5), np.log(2.0), size=n))[:, None, None]
+    iP = np.ascontiguousarray(1j * H * scale)
+    c1 = 0.5 * np.sum(np.abs(H * scale) ** 2, axis=(1, 2))
+    assert (c1 < 1e-4).any() and ((c1 > 1e-4) & (c1 < 0.25)).any() and (c1 > 0.25).any()
+    ref = np.array([sl.expm(m) for m in iP])
+    out = ctx.exp_su3(iP.view(np.float64).reshape(n, 18), FP64).reshape(n, 9, 2)
+    got = (out[..., 0] + 1j * out[..., 1]).reshape(n, 3, 3)
+    assert np.max(np.abs(got - ref)) < 5e-15
+
+
 def test_exp_zero_is_identity(ctx):
     out = ctx.exp_su3(np.zeros((3, 18)), FP64).reshape(-1, 9, 2)
     assert np.array_equal(out[:, :, 0], np.tile(np.eye(3).reshape(9), (3, 1)))
