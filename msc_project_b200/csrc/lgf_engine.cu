@@ -135,7 +135,9 @@ public:
         int nb = 0;
         LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rk3_stage<R, 1>, threads_, 0));
         stage_grid_max_ = std::max(1, nb) * ctx_->sm_count;
-        LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R>, MEAS_SITES * 6, 0));
+        LGF_CUDA_TRY(ctx_, prepare_measure_kernel<R>());
+        LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R>, MEAS_SITES * 6,
+                                                                         measure_smem_bytes<R>()));
         meas_grid_max_ = std::max(1, nb) * ctx_->sm_count;
         if (dynamic_) {
             // members change after capture: size the measurement lists for the
@@ -273,8 +275,8 @@ public:
             if (k == 1) k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
             if (k == 2) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
         } else {
-            k_measure<R><<<meas_grid(), dim3(MEAS_SITES, 6), 0, ctx_->stream>>>(d_desc_, d_mtiles_, d_counts_ + 1,
-                                                                             nullptr, nullptr);
+            k_measure<R><<<meas_grid(), dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+                d_desc_, d_mtiles_, d_counts_ + 1, nullptr, nullptr, nullptr, nullptr);
         }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
@@ -284,7 +286,8 @@ public:
         const int mg = meas_grid();
         const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
         const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
-        k_measure<R><<<mg, dim3(MEAS_SITES, 6), 0, ctx_->stream>>>(d_desc_, d_mtiles_, d_counts_ + 1, nullptr, nullptr);
+        k_measure<R><<<mg, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+            d_desc_, d_mtiles_, d_counts_ + 1, nullptr, nullptr, nullptr, nullptr);
         k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
         k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
@@ -514,9 +517,46 @@ struct lgf_lattice {
     double last_flow_s = 0.0;
 };
 
-template <typename R> static void launch_site_meas(lgf_ctx* ctx, LatticeBuf& b, double* se, double* sq, LatDesc<R>* d_desc,
-                                                  int4* d_mt, int* d_n, int n) {
-    k_measure<R><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, 6), 0, ctx->stream>>>(d_desc, d_mt, d_n, se, sq);
+// One measurement-kernel pass over a single lattice with per-site (and,
+// when asked, per (site, plane) F / F^) outputs; no reduction.
+template <typename R>
+static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, double* dev_q, double2* dbg_c,
+                                  double2* dbg_i) {
+    std::vector<int4> mt;
+    for (int t = 0; t < b.g.n[0]; ++t)
+        for (int c = 0; c < b.nchunk; ++c) mt.push_back(make_int4(0, t, c, 0));
+    const int n = (int)mt.size();
+    LatDesc<R> d{};
+    d.g = b.g;
+    d.U0 = (cplx<R>*)b.U[0];
+    d.partial = b.partial;
+    d.nchunk = b.nchunk;
+    void* ddesc = nullptr;
+    int4* dmt = nullptr;
+    int* dn = nullptr;
+    cudaError_t e = prepare_measure_kernel<R>();
+    if (e == cudaSuccess) e = cudaMalloc(&ddesc, sizeof d);
+    if (e == cudaSuccess) e = cudaMalloc(&dmt, sizeof(int4) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dn, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ddesc, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmt, mt.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        k_measure<R><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx->stream>>>(
+            (const LatDesc<R>*)ddesc, dmt, dn, dev_e, dev_q, dbg_c, dbg_i);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(ddesc);
+    cudaFree(dmt);
+    cudaFree(dn);
+    if (e != cudaSuccess) return set_error(ctx, LGF_ECUDA, "measurement pass failed: %s", cudaGetErrorString(e));
+    return LGF_OK;
+}
+
+static int single_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, double* dev_q, double2* dbg_c, double2* dbg_i) {
+    return b.prec == LGF_PREC_FP64 ? single_lattice_measure<double>(ctx, b, dev_e, dev_q, dbg_c, dbg_i)
+                                   : single_lattice_measure<float>(ctx, b, dev_e, dev_q, dbg_c, dbg_i);
 }
 
 // =================================================================== C ABI
@@ -755,50 +795,15 @@ int lgf_site_densities(lgf_lattice* lat, double* e_site, double* q_site) {
     LatticeBuf& b = lat->buf;
     const size_t V = (size_t)b.g.V;
     double *de = nullptr, *dq = nullptr;
-    void* ddesc = nullptr;
-    int4* dmt = nullptr;
-    int* dn = nullptr;
-    std::vector<int4> mt;
-    for (int t = 0; t < b.g.n[0]; ++t)
-        for (int c = 0; c < b.nchunk; ++c) mt.push_back(make_int4(0, t, c, 0));
-    const int n = (int)mt.size();
-    int rc = LGF_OK;
-    cudaError_t e = cudaMalloc(&de, V * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&dq, V * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&ddesc, sizeof(LatDesc<double>));
-    if (e == cudaSuccess) e = cudaMalloc(&dmt, sizeof(int4) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dn, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dmt, mt.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) {
-        if (b.prec == LGF_PREC_FP64) {
-            LatDesc<double> d{};
-            d.g = b.g;
-            d.U0 = (cplx<double>*)b.U[0];
-            d.partial = b.partial;
-            d.nchunk = b.nchunk;
-            e = cudaMemcpyAsync(ddesc, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream);
-            if (e == cudaSuccess) launch_site_meas<double>(ctx, b, de, dq, (LatDesc<double>*)ddesc, dmt, dn, n);
-        } else {
-            LatDesc<float> d{};
-            d.g = b.g;
-            d.U0 = (cplx<float>*)b.U[0];
-            d.partial = b.partial;
-            d.nchunk = b.nchunk;
-            e = cudaMemcpyAsync(ddesc, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream);
-            if (e == cudaSuccess) launch_site_meas<float>(ctx, b, de, dq, (LatDesc<float>*)ddesc, dmt, dn, n);
-        }
-        if (e == cudaSuccess) e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && e_site) e = cudaMemcpyAsync(e_site, de, V * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess && q_site) e = cudaMemcpyAsync(q_site, dq, V * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "site densities failed: %s", cudaGetErrorString(e));
+    LGF_CUDA_TRY(ctx, cudaMalloc(&de, V * sizeof(double)));
+    cudaError_t e = cudaMalloc(&dq, V * sizeof(double));
+    int rc = e == cudaSuccess ? single_measure(ctx, b, de, dq, nullptr, nullptr)
+                              : set_error(ctx, LGF_ENOMEM, "site density buffers: %s", cudaGetErrorString(e));
+    if (rc == LGF_OK && e_site) e = cudaMemcpy(e_site, de, V * sizeof(double), cudaMemcpyDeviceToHost);
+    if (rc == LGF_OK && e == cudaSuccess && q_site) e = cudaMemcpy(q_site, dq, V * sizeof(double), cudaMemcpyDeviceToHost);
+    if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "site densities copy: %s", cudaGetErrorString(e));
     cudaFree(de);
     cudaFree(dq);
-    cudaFree(ddesc);
-    cudaFree(dmt);
-    cudaFree(dn);
     return rc;
 }
 
@@ -898,25 +903,19 @@ int lgf_debug_fields(lgf_lattice* lat, double* clover_F, double* improved_F) {
     if (!lat) return LGF_EINVAL;
     lgf_ctx* ctx = lat->ctx;
     cudaSetDevice(ctx->device);
-    const LatticeBuf& b = lat->buf;
+    LatticeBuf& b = lat->buf;
     const size_t bytes = (size_t)b.g.V * 6 * 18 * sizeof(double);
     double2 *dc = nullptr, *di = nullptr;
     LGF_CUDA_TRY(ctx, cudaMalloc(&dc, bytes));
     cudaError_t e = cudaMalloc(&di, bytes);
-    if (e == cudaSuccess) {
-        if (b.prec == LGF_PREC_FP64)
-            k_debug_fields<double><<<blocks_for(6LL * b.g.V, 64), 64, 0, ctx->stream>>>((const cplx<double>*)b.U[0], b.g, dc, di);
-        else
-            k_debug_fields<float><<<blocks_for(6LL * b.g.V, 64), 64, 0, ctx->stream>>>((const cplx<float>*)b.U[0], b.g, dc, di);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && clover_F) e = cudaMemcpyAsync(clover_F, dc, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess && improved_F) e = cudaMemcpyAsync(improved_F, di, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    int rc = e == cudaSuccess ? single_measure(ctx, b, nullptr, nullptr, dc, di)
+                              : set_error(ctx, LGF_ENOMEM, "debug field buffers: %s", cudaGetErrorString(e));
+    if (rc == LGF_OK && clover_F) e = cudaMemcpy(clover_F, dc, bytes, cudaMemcpyDeviceToHost);
+    if (rc == LGF_OK && e == cudaSuccess && improved_F) e = cudaMemcpy(improved_F, di, bytes, cudaMemcpyDeviceToHost);
+    if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "debug fields copy: %s", cudaGetErrorString(e));
     cudaFree(dc);
     cudaFree(di);
-    if (e != cudaSuccess) return set_error(ctx, LGF_ECUDA, "debug fields failed: %s", cudaGetErrorString(e));
-    return LGF_OK;
+    return rc;
 }
 
 int lgf_exp_su3(lgf_ctx* ctx, int precision, const double* iP, double* out, long long n) {

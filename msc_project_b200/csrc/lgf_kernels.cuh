@@ -186,6 +186,20 @@ template <typename R> struct Plane {
             for (int c = 0; c < 3; ++c) a.m[3 * r + c] = cmk<R>(l.m[3 * c + r].re, -l.m[3 * c + r].im);
         return a;
     }
+    // move p by count steps without loading links
+    __device__ __forceinline__ void advance(PlanePos& p, bool along_mu, int sign, int count) const {
+        const Dir& d = along_mu ? dm : dn;
+        int& xc = along_mu ? p.xm : p.xn;
+        for (int i = 0; i < count; ++i) {
+            if (sign > 0) {
+                p.s = (xc == d.n - 1) ? p.s - (d.n - 1) * d.stride : p.s + d.stride;
+                xc = wrap_inc(xc, d.n);
+            } else {
+                p.s = (xc == 0) ? p.s + (d.n - 1) * d.stride : p.s - d.stride;
+                xc = wrap_dec(xc, d.n);
+            }
+        }
+    }
     // P <- P * (link of one step from p)
     __device__ __forceinline__ void ext(su3<R>& P, PlanePos& p, bool along_mu, int sign) const {
         const Dir& d = along_mu ? dm : dn;
@@ -237,9 +251,68 @@ template <typename R> __device__ __forceinline__ void leaf_acc(const su3<R>& A, 
     }
 }
 
+template <typename R> __device__ __forceinline__ void store_alg_as_antiherm(double2* dst, const alg<R>& z) {
+    const double v0 = z.v[0], v1 = z.v[1];
+    dst[0] = make_double2(0.0, v0);
+    dst[4] = make_double2(0.0, v1);
+    dst[8] = make_double2(0.0, -(v0 + v1));
+    dst[1] = make_double2(z.v[2], z.v[3]);
+    dst[3] = make_double2(-(double)z.v[2], z.v[3]);
+    dst[2] = make_double2(z.v[4], z.v[5]);
+    dst[6] = make_double2(-(double)z.v[4], z.v[5]);
+    dst[5] = make_double2(z.v[6], z.v[7]);
+    dst[7] = make_double2(-(double)z.v[6], z.v[7]);
+}
+template <typename R> __device__ __forceinline__ void store_alg_as_herm(double2* dst, const alg<R>& f) {
+    const double v0 = f.v[0], v1 = f.v[1];
+    dst[0] = make_double2(v0, 0.0);
+    dst[4] = make_double2(v1, 0.0);
+    dst[8] = make_double2(-(v0 + v1), 0.0);
+    dst[1] = make_double2(f.v[2], f.v[3]);
+    dst[3] = make_double2(f.v[2], -(double)f.v[3]);
+    dst[2] = make_double2(f.v[4], f.v[5]);
+    dst[6] = make_double2(f.v[4], -(double)f.v[5]);
+    dst[5] = make_double2(f.v[6], f.v[7]);
+    dst[7] = make_double2(f.v[6], -(double)f.v[7]);
+}
+
+__device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
+__device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
+
+constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
+
+// Shared memory of one measurement block: the straight lines of length 2 and
+// 3 from each of its 32 sites in the 8 signed directions (every plane and
+// quadrant of the site reuses them), then the per-plane results.
+template <typename R> struct MeasSmem {
+    R line[8][2][18][MEAS_SITES];  // [2*dir + (sign<0)][length-2][entry][site]
+    alg<R> F[6][MEAS_SITES];
+    double E[6][MEAS_SITES];
+};
+
 template <typename R>
-__device__ __forceinline__ void plane_fields(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
-                                             int mu, int nu, alg<R>& F11, alg<R>& Fhat) {
+__device__ __forceinline__ void store_line(MeasSmem<R>* sm, int sdir, int len, int lane, const su3<R>& L) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        sm->line[sdir][len - 2][2 * k][lane] = L.m[k].re;
+        sm->line[sdir][len - 2][2 * k + 1][lane] = L.m[k].im;
+    }
+}
+template <typename R>
+__device__ __forceinline__ su3<R> load_line(const MeasSmem<R>* sm, int sdir, int len, int lane) {
+    su3<R> L;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) L.m[k] = cmk<R>(sm->line[sdir][len - 2][2 * k][lane], sm->line[sdir][len - 2][2 * k + 1][lane]);
+    return L;
+}
+
+// Clover F and improved F of plane (mu, nu) at the thread's site, using the
+// block's shared lines (21 matrix products and 16 global link loads per
+// quadrant).  See the comment above Plane for the leaf decomposition.
+template <typename R>
+__device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                                  int mu, int nu, const MeasSmem<R>* sm, int lane, alg<R>& F11,
+                                                  alg<R>& Fhat) {
     Plane<R> P;
     P.U = U;
     P.V = g.V;
@@ -249,80 +322,76 @@ __device__ __forceinline__ void plane_fields(const cplx<R>* __restrict__ U, cons
     P.dn = dir_of(g, c, nu);
     const PlanePos x0 = {s, P.dm.x, P.dn.x};
     const R k11 = R(19.0 / 36.0), k12 = R(-4.0 / 45.0), k13 = R(1.0 / 120.0), k22 = R(1.0 / 144.0);
+    alg<R> G;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        F11.v[k] = R(0);
+        G.v[k] = R(0);
         Fhat.v[k] = R(0);
     }
-    alg<R> G;  // 1x1 leaves, for both F and F^
-#pragma unroll
-    for (int k = 0; k < 8; ++k) G.v[k] = R(0);
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
-        const int sm = (q == 0 || q == 1) ? 1 : -1;
+        const int sm_ = (q == 0 || q == 1) ? 1 : -1;
         const int sn = (q == 0 || q == 2) ? 1 : -1;
         const R sg = (q == 0 || q == 3) ? R(1) : R(-1);
-        // row: shapes (1,1), (2,1), (3,1)
-        PlanePos pn = x0, pm = x0;
-        su3<R> Rn = P.step(pn, false, sn);  // (sn nu)
-        su3<R> Lm = P.step(pm, true, sm);   // (sm mu)
-        P.ext(Rn, pn, true, sm);            // Pn(1,1)
+        const int sdm = 2 * mu + (sm_ < 0 ? 1 : 0), sdn = 2 * nu + (sn < 0 ? 1 : 0);
+        // row: (1,1), (2,1), (3,1)
+        PlanePos pn = x0;
+        su3<R> Rn = P.step(pn, false, sn);
+        P.ext(Rn, pn, true, sm_);  // Pn(1,1)
         {
-            PlanePos q2 = pm;
-            su3<R> Pm = Lm;
-            P.ext(Pm, q2, false, sn);        // Pm(1,1)
+            PlanePos q2 = x0;
+            su3<R> Pm = P.step(q2, true, sm_);
+            P.ext(Pm, q2, false, sn);  // Pm(1,1)
             leaf_acc(Rn, Pm, sg, G);
         }
-        P.ext(Rn, pn, true, sm);            // Pn(2,1)
-        P.ext(Lm, pm, true, sm);            // (sm mu)^2
+        P.ext(Rn, pn, true, sm_);  // Pn(2,1)
         {
-            PlanePos q2 = pm;
-            su3<R> Pm = Lm;
-            P.ext(Pm, q2, false, sn);        // Pm(2,1)
+            PlanePos q2 = x0;
+            P.advance(q2, true, sm_, 2);
+            su3<R> Pm = load_line(sm, sdm, 2, lane);
+            P.ext(Pm, q2, false, sn);  // Pm(2,1)
             leaf_acc(Rn, Pm, sg * k12, Fhat);
         }
-        P.ext(Rn, pn, true, sm);            // Pn(3,1)
-        P.ext(Lm, pm, true, sm);            // (sm mu)^3
+        P.ext(Rn, pn, true, sm_);  // Pn(3,1)
         {
-            PlanePos q2 = pm;
-            su3<R> Pm = Lm;
-            P.ext(Pm, q2, false, sn);        // Pm(3,1)
+            PlanePos q2 = x0;
+            P.advance(q2, true, sm_, 3);
+            su3<R> Pm = load_line(sm, sdm, 3, lane);
+            P.ext(Pm, q2, false, sn);  // Pm(3,1)
             leaf_acc(Rn, Pm, sg * k13, Fhat);
         }
-        // column: shapes (1,2), (1,3)
-        pn = x0;
-        Rn = P.step(pn, false, sn);
-        P.ext(Rn, pn, false, sn);           // (sn nu)^2
-        pm = x0;
-        Lm = P.step(pm, true, sm);
-        P.ext(Lm, pm, false, sn);
-        P.ext(Lm, pm, false, sn);           // Pm(1,2)
+        // column: (1,2), (1,3)
         {
-            PlanePos q2 = pn;
-            su3<R> Pn = Rn;
-            P.ext(Pn, q2, true, sm);         // Pn(1,2)
+            PlanePos qm = x0;
+            su3<R> Lm = P.step(qm, true, sm_);
+            P.ext(Lm, qm, false, sn);
+            P.ext(Lm, qm, false, sn);  // Pm(1,2)
+            PlanePos q2 = x0;
+            P.advance(q2, false, sn, 2);
+            su3<R> Pn = load_line(sm, sdn, 2, lane);
+            P.ext(Pn, q2, true, sm_);  // Pn(1,2)
             leaf_acc(Pn, Lm, sg * k12, Fhat);
-        }
-        P.ext(Rn, pn, false, sn);           // (sn nu)^3
-        P.ext(Lm, pm, false, sn);           // Pm(1,3)
-        {
-            PlanePos q2 = pn;
-            su3<R> Pn = Rn;
-            P.ext(Pn, q2, true, sm);         // Pn(1,3)
+            P.ext(Lm, qm, false, sn);  // Pm(1,3)
+            PlanePos q3 = x0;
+            P.advance(q3, false, sn, 3);
+            Pn = load_line(sm, sdn, 3, lane);
+            P.ext(Pn, q3, true, sm_);  // Pn(1,3)
             leaf_acc(Pn, Lm, sg * k13, Fhat);
         }
         // (2,2)
-        pn = x0;
-        Rn = P.step(pn, false, sn);
-        P.ext(Rn, pn, false, sn);
-        P.ext(Rn, pn, true, sm);
-        P.ext(Rn, pn, true, sm);            // Pn(2,2)
-        pm = x0;
-        Lm = P.step(pm, true, sm);
-        P.ext(Lm, pm, true, sm);
-        P.ext(Lm, pm, false, sn);
-        P.ext(Lm, pm, false, sn);           // Pm(2,2)
-        leaf_acc(Rn, Lm, sg * k22, Fhat);
+        {
+            PlanePos q2 = x0;
+            P.advance(q2, false, sn, 2);
+            su3<R> Pn = load_line(sm, sdn, 2, lane);
+            P.ext(Pn, q2, true, sm_);
+            P.ext(Pn, q2, true, sm_);  // Pn(2,2)
+            PlanePos qm = x0;
+            P.advance(qm, true, sm_, 2);
+            su3<R> Pm = load_line(sm, sdm, 2, lane);
+            P.ext(Pm, qm, false, sn);
+            P.ext(Pm, qm, false, sn);  // Pm(2,2)
+            leaf_acc(Pn, Pm, sg * k22, Fhat);
+        }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -331,26 +400,28 @@ __device__ __forceinline__ void plane_fields(const cplx<R>* __restrict__ U, cons
     }
 }
 
-__device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
-__device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
-
-constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
-
 // Measurement tile = (lattice, x0 slice, chunk of 32 consecutive sites of the
-// slice); 6 warps = 6 planes.  Writes the tile's sums of e(x) and q(x) to the
-// lattice's partial[slice * nchunk + chunk] (double2) and, when site_e/site_q
-// are not null (single-lattice use), e(x) and q(x) per site.
+// slice); 6 warps = 6 planes.  Phase 0: the block's lines (warp w builds the
+// lines of signed direction w, and w+6 for w < 2) into shared memory.  Phase
+// 1: F and F^ of every (site, plane).  Phase 2: the six planes meet in shared
+// memory for e(x) and q(x); the tile's sums go to the lattice's
+// partial[slice * nchunk + chunk] (double2).  site_e/site_q (single-lattice
+// use) receive e(x), q(x) per site; dbg_clover/dbg_improved receive F and F^
+// per (site, plane) as Hermitian 3x3 matrices (parity tests).
 //   e(x) = sum_{mu<nu} ReTr(F F)                 (EnergyDensity.cpp:13-20)
 //   q(x) = ReTr(F^32 F^01) + ReTr(F^31 F^20) + ReTr(F^30 F^12)
 //        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
 //                                             (TopologicalCharge.cpp:11-16)
 template <typename R>
 __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const LatDesc<R>* __restrict__ descs,
-                                                            const int4* __restrict__ mtiles,
-                                                            const int* __restrict__ nmtiles,
-                                                            double* __restrict__ site_e, double* __restrict__ site_q) {
-    __shared__ alg<R> sF[6][MEAS_SITES];
-    __shared__ double sE[6][MEAS_SITES];
+                                                                           const int4* __restrict__ mtiles,
+                                                                           const int* __restrict__ nmtiles,
+                                                                           double* __restrict__ site_e,
+                                                                           double* __restrict__ site_q,
+                                                                           double2* __restrict__ dbg_clover,
+                                                                           double2* __restrict__ dbg_improved) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MeasSmem<R>* sm = reinterpret_cast<MeasSmem<R>*>(smem_raw);
     const int lane = threadIdx.x, p = threadIdx.y;
     const int n = *nmtiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
@@ -361,20 +432,46 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const
         const int off = chunk * MEAS_SITES + lane;
         const bool valid = off < g.Vs;
         const int s = slice * g.Vs + (valid ? off : 0);
-        if (valid) {
-            const Coord c = site_coord(g, s);
-            alg<R> F11, Fh;
-            plane_fields<R>(d->U0, g, s, c, c_plane_mu[p], c_plane_nu[p], F11, Fh);
-            sF[p][lane] = Fh;
-            sE[p][lane] = retr_hh(F11, F11);
+        const Coord c = site_coord(g, s);
+        const cplx<R>* __restrict__ U = d->U0;
+        // phase 0: lines of length 2 and 3 in the 8 signed directions
+        for (int sdir = p; sdir < 8; sdir += 6) {
+            const int dir = sdir >> 1, sign = (sdir & 1) ? -1 : 1;
+            Plane<R> L;
+            L.U = U;
+            L.V = g.V;
+            L.mu = dir;
+            L.nu = dir;
+            L.dm = dir_of(g, c, dir);
+            L.dn = L.dm;
+            PlanePos y = {s, L.dm.x, L.dm.x};
+            su3<R> acc = L.step(y, true, sign);
+            L.ext(acc, y, true, sign);
+            store_line(sm, sdir, 2, lane, acc);
+            L.ext(acc, y, true, sign);
+            store_line(sm, sdir, 3, lane, acc);
         }
         __syncthreads();
+        // phase 1: this thread's plane
+        if (valid) {
+            alg<R> F11, Fh;
+            plane_fields_smem<R>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, F11, Fh);
+            sm->F[p][lane] = Fh;
+            sm->E[p][lane] = retr_hh(F11, F11);
+            if (dbg_clover) {
+                store_alg_as_herm(dbg_clover + ((size_t)s * 6 + p) * 9, F11);
+                store_alg_as_herm(dbg_improved + ((size_t)s * 6 + p) * 9, Fh);
+            }
+        }
+        __syncthreads();
+        // phase 2: the site's e(x), q(x) and the tile's sums
         if (p == 0) {
             double e = 0.0, q = 0.0;
             if (valid) {
-                e = ((sE[0][lane] + sE[1][lane]) + (sE[2][lane] + sE[3][lane])) + (sE[4][lane] + sE[5][lane]);
-                q = -retr_hh(sF[5][lane], sF[0][lane]) + retr_hh(sF[4][lane], sF[1][lane]) -
-                    retr_hh(sF[2][lane], sF[3][lane]);
+                e = ((sm->E[0][lane] + sm->E[1][lane]) + (sm->E[2][lane] + sm->E[3][lane])) +
+                    (sm->E[4][lane] + sm->E[5][lane]);
+                q = -retr_hh(sm->F[5][lane], sm->F[0][lane]) + retr_hh(sm->F[4][lane], sm->F[1][lane]) -
+                    retr_hh(sm->F[2][lane], sm->F[3][lane]);
                 if (site_e) site_e[s] = e;
                 if (site_q) site_q[s] = q;
             }
@@ -387,6 +484,13 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const
         }
         __syncthreads();
     }
+}
+
+// Dynamic shared memory of k_measure<R> (above 48 KB for double: the
+// attribute must be raised once per device before the first launch).
+template <typename R> inline size_t measure_smem_bytes() { return sizeof(MeasSmem<R>); }
+template <typename R> inline cudaError_t prepare_measure_kernel() {
+    return cudaFuncSetAttribute(k_measure<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MeasSmem<R>));
 }
 
 constexpr int RED_THREADS = 256;
@@ -628,31 +732,6 @@ __global__ void __launch_bounds__(256) k_unitarity(const cplx<R>* __restrict__ U
 }
 
 // ---------------------------------------------------- per-function debug
-template <typename R> __device__ __forceinline__ void store_alg_as_antiherm(double2* dst, const alg<R>& z) {
-    const double v0 = z.v[0], v1 = z.v[1];
-    dst[0] = make_double2(0.0, v0);
-    dst[4] = make_double2(0.0, v1);
-    dst[8] = make_double2(0.0, -(v0 + v1));
-    dst[1] = make_double2(z.v[2], z.v[3]);
-    dst[3] = make_double2(-(double)z.v[2], z.v[3]);
-    dst[2] = make_double2(z.v[4], z.v[5]);
-    dst[6] = make_double2(-(double)z.v[4], z.v[5]);
-    dst[5] = make_double2(z.v[6], z.v[7]);
-    dst[7] = make_double2(-(double)z.v[6], z.v[7]);
-}
-template <typename R> __device__ __forceinline__ void store_alg_as_herm(double2* dst, const alg<R>& f) {
-    const double v0 = f.v[0], v1 = f.v[1];
-    dst[0] = make_double2(v0, 0.0);
-    dst[4] = make_double2(v1, 0.0);
-    dst[8] = make_double2(-(v0 + v1), 0.0);
-    dst[1] = make_double2(f.v[2], f.v[3]);
-    dst[3] = make_double2(f.v[2], -(double)f.v[3]);
-    dst[2] = make_double2(f.v[4], f.v[5]);
-    dst[6] = make_double2(f.v[4], -(double)f.v[5]);
-    dst[5] = make_double2(f.v[6], f.v[7]);
-    dst[7] = make_double2(f.v[6], -(double)f.v[7]);
-}
-
 // flow gradient Z(x, mu) for every link, file order [s][mu][9] (double2)
 template <typename R>
 __global__ void k_debug_gradient(const cplx<R>* __restrict__ U, Geom g, double2* __restrict__ out) {
@@ -663,20 +742,6 @@ __global__ void k_debug_gradient(const cplx<R>* __restrict__ U, Geom g, double2*
     su3<R> u;
     const alg<R> Z = flow_gradient<R>(U, g, s, c, mu, u);
     store_alg_as_antiherm(out + ((size_t)s * 4 + mu) * 9, Z);
-}
-
-// clover F and improved F for every (site, plane (01,02,03,12,13,23)), [s][p][9]
-template <typename R>
-__global__ void k_debug_fields(const cplx<R>* __restrict__ U, Geom g, double2* __restrict__ clover,
-                               double2* __restrict__ improved) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 6 * g.V) return;
-    const int p = t / g.V, s = t - p * g.V;
-    const Coord c = site_coord(g, s);
-    alg<R> F11, Fh;
-    plane_fields<R>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], F11, Fh);
-    store_alg_as_herm(clover + ((size_t)s * 6 + p) * 9, F11);
-    store_alg_as_herm(improved + ((size_t)s * 6 + p) * 9, Fh);
 }
 
 // exp(iP) for n anti-Hermitian traceless matrices given as full 3x3 (double2)
