@@ -105,6 +105,11 @@ int lgf_measure(lgf_lattice* lat, double* E, double* Q, double* E_slice, double*
 /* per-site e(x) = sum_{mu<nu} ReTr(F F) (clover F) and q(x) (improved F,
  * before the 1/(4 pi^2)), [V] each in global site order; either may be NULL */
 int lgf_site_densities(lgf_lattice* lat, double* e_site, double* q_site);
+/* The observables of MeasureFlowedGaugeConfigurations (LGF/LGF.cpp:228-255):
+ * E with the improved F (ImprovedEnergyDensity::calculate,
+ * LGF/Observables/ImprovedEnergyDensity.cpp:9-34) and Q with the clover F
+ * (UnImprovedTopologicalCharge::calculate, UnImprovedTopologicalCharge.cpp:8-29). */
+int lgf_measure_flowed(lgf_lattice* lat, double* E_improved, double* Q_clover);
 /* max over links of ||U^dag U - 1||_F and |det U - 1| */
 int lgf_unitarity(lgf_lattice* lat, double* max_unit_err, double* max_det_err);
 

@@ -12,6 +12,8 @@
  *       (LGF/LGF.h:32, LGF/LGF.cpp:197-226)
  *   void MeasureQdensityDistribution(SimulationParameters&, FlowParameters&)
  *       (LGF/LGF.h:35, LGF/LGF.cpp:114-124)
+ *   void MeasureFlowedGaugeConfigurations(SimulationParameters&, FlowParameters&)
+ *       (LGF/LGF.h:34, LGF/LGF.cpp:228-255)
  * with the same input/output files (ensembles/.../*.bin, Observables/.../*.csv)
  * and the same stdout lines; the flow and the measurements run on the GPU
  * through lgf_b200.h.  Other languages bind the extern "C" functions at the end.
@@ -75,6 +77,7 @@ private:
 void FlowSavedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams);
 void ResumeFlowedConfiguration(SimulationParameters& params, FlowParameters& flowParams, double flowTime_pickup);
 void MeasureQdensityDistribution(SimulationParameters& params, FlowParameters& flowParams);
+void MeasureFlowedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams);
 
 extern "C" {
 #endif
@@ -92,6 +95,8 @@ int lgf_dropin_resume_flowed(const int shape[4], double beta, int config_start, 
                              double epsilon, int measure_every, const char* data_folder, double flow_time_pickup);
 int lgf_dropin_measure_qdensity(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
                                 double epsilon, int measure_every, const char* data_folder);
+int lgf_dropin_measure_flowed(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
+                              double epsilon, int measure_every, const char* data_folder);
 
 #ifdef __cplusplus
 }

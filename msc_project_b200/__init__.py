@@ -7,5 +7,5 @@ Python mirror for tests and benchmarks.
 """
 from ._capi import LIB_PATH, load  # noqa: F401
 from .lgf import (FP32MIXED, FP64, Context, FlowParameters, FlowResult, FlowSavedGaugeConfigurations,  # noqa: F401
-                  Job, Lattice, LGFError, MeasureQdensityDistribution, ResumeFlowedConfiguration, Server,
+                  Job, Lattice, LGFError, MeasureFlowedGaugeConfigurations, MeasureQdensityDistribution, ResumeFlowedConfiguration, Server,
                   SimulationParameters, configure, volume)

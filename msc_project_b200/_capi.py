@@ -76,6 +76,7 @@ SIGNATURES = {
     "lgf_measure": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
     "lgf_site_densities": (ctypes.c_int, [_vp, _dp, _dp]),
     "lgf_unitarity": (ctypes.c_int, [_vp, _dp, _dp]),
+    "lgf_measure_flowed": (ctypes.c_int, [_vp, _dp, _dp]),
     "lgf_debug_gradient": (ctypes.c_int, [_vp, _dp]),
     "lgf_debug_fields": (ctypes.c_int, [_vp, _dp, _dp]),
     "lgf_exp_su3": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, ctypes.c_longlong]),
@@ -94,6 +95,8 @@ SIGNATURES = {
                                              ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
     "lgf_dropin_resume_flowed": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_double]),
+    "lgf_dropin_measure_flowed": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
     "lgf_dropin_measure_qdensity": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
 }

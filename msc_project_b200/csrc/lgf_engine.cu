@@ -276,7 +276,7 @@ public:
             if (k == 2) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
         } else {
             k_measure<R><<<meas_grid(), dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
-                d_desc_, d_mtiles_, d_counts_ + 1, nullptr, nullptr, nullptr, nullptr);
+                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
         }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
@@ -287,7 +287,7 @@ public:
         const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
         const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
         k_measure<R><<<mg, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
-            d_desc_, d_mtiles_, d_counts_ + 1, nullptr, nullptr, nullptr, nullptr);
+            d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
         k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
         k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
@@ -519,9 +519,7 @@ struct lgf_lattice {
 
 // One measurement-kernel pass over a single lattice with per-site (and,
 // when asked, per (site, plane) F / F^) outputs; no reduction.
-template <typename R>
-static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, double* dev_q, double2* dbg_c,
-                                  double2* dbg_i) {
+template <typename R> static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, const MeasOut& out) {
     std::vector<int4> mt;
     for (int t = 0; t < b.g.n[0]; ++t)
         for (int c = 0; c < b.nchunk; ++c) mt.push_back(make_int4(0, t, c, 0));
@@ -534,7 +532,7 @@ static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, do
     void* ddesc = nullptr;
     int4* dmt = nullptr;
     int* dn = nullptr;
-    cudaError_t e = prepare_measure_kernel<R>();
+    cudaError_t e = prepare_measure_kernel<R, true>();
     if (e == cudaSuccess) e = cudaMalloc(&ddesc, sizeof d);
     if (e == cudaSuccess) e = cudaMalloc(&dmt, sizeof(int4) * n);
     if (e == cudaSuccess) e = cudaMalloc(&dn, sizeof(int));
@@ -542,8 +540,8 @@ static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, do
     if (e == cudaSuccess) e = cudaMemcpyAsync(dmt, mt.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        k_measure<R><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx->stream>>>(
-            (const LatDesc<R>*)ddesc, dmt, dn, dev_e, dev_q, dbg_c, dbg_i);
+        k_measure<R, true><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, 6), measure_smem_bytes<R, true>(),
+                             ctx->stream>>>((const LatDesc<R>*)ddesc, dmt, dn, out);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -554,9 +552,9 @@ static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, do
     return LGF_OK;
 }
 
-static int single_measure(lgf_ctx* ctx, LatticeBuf& b, double* dev_e, double* dev_q, double2* dbg_c, double2* dbg_i) {
-    return b.prec == LGF_PREC_FP64 ? single_lattice_measure<double>(ctx, b, dev_e, dev_q, dbg_c, dbg_i)
-                                   : single_lattice_measure<float>(ctx, b, dev_e, dev_q, dbg_c, dbg_i);
+static int single_measure(lgf_ctx* ctx, LatticeBuf& b, const MeasOut& out) {
+    return b.prec == LGF_PREC_FP64 ? single_lattice_measure<double>(ctx, b, out)
+                                   : single_lattice_measure<float>(ctx, b, out);
 }
 
 // =================================================================== C ABI
@@ -797,7 +795,10 @@ int lgf_site_densities(lgf_lattice* lat, double* e_site, double* q_site) {
     double *de = nullptr, *dq = nullptr;
     LGF_CUDA_TRY(ctx, cudaMalloc(&de, V * sizeof(double)));
     cudaError_t e = cudaMalloc(&dq, V * sizeof(double));
-    int rc = e == cudaSuccess ? single_measure(ctx, b, de, dq, nullptr, nullptr)
+    MeasOut mo{};
+    mo.e = de;
+    mo.q = dq;
+    int rc = e == cudaSuccess ? single_measure(ctx, b, mo)
                               : set_error(ctx, LGF_ENOMEM, "site density buffers: %s", cudaGetErrorString(e));
     if (rc == LGF_OK && e_site) e = cudaMemcpy(e_site, de, V * sizeof(double), cudaMemcpyDeviceToHost);
     if (rc == LGF_OK && e == cudaSuccess && q_site) e = cudaMemcpy(q_site, dq, V * sizeof(double), cudaMemcpyDeviceToHost);
@@ -805,6 +806,39 @@ int lgf_site_densities(lgf_lattice* lat, double* e_site, double* q_site) {
     cudaFree(de);
     cudaFree(dq);
     return rc;
+}
+
+int lgf_measure_flowed(lgf_lattice* lat, double* E_improved, double* Q_clover) {
+    if (!lat) return LGF_EINVAL;
+    lgf_ctx* ctx = lat->ctx;
+    cudaSetDevice(ctx->device);
+    LatticeBuf& b = lat->buf;
+    const size_t V = (size_t)b.g.V;
+    double *de = nullptr, *dq = nullptr;
+    LGF_CUDA_TRY(ctx, cudaMalloc(&de, V * sizeof(double)));
+    cudaError_t e = cudaMalloc(&dq, V * sizeof(double));
+    MeasOut mo{};
+    mo.e_imp = de;
+    mo.q_clov = dq;
+    int rc = e == cudaSuccess ? single_measure(ctx, b, mo)
+                              : set_error(ctx, LGF_ENOMEM, "density buffers: %s", cudaGetErrorString(e));
+    std::vector<double> he(V), hq(V);
+    if (rc == LGF_OK) e = cudaMemcpy(he.data(), de, V * sizeof(double), cudaMemcpyDeviceToHost);
+    if (rc == LGF_OK && e == cudaSuccess) e = cudaMemcpy(hq.data(), dq, V * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(de);
+    cudaFree(dq);
+    if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "density copy: %s", cudaGetErrorString(e));
+    if (rc != LGF_OK) return rc;
+    // fixed-order sums in global site order (ImprovedEnergyDensity.cpp:26, UnImprovedTopologicalCharge.cpp:21)
+    double se = 0.0, sq = 0.0;
+    for (size_t i = 0; i < V; ++i) {
+        se += he[i];
+        sq += hq[i];
+    }
+    const double PI = 3.14159265358979323846;
+    if (E_improved) *E_improved = se * (1.0 / (double)V);
+    if (Q_clover) *Q_clover = sq * (1.0 / (4.0 * PI * PI));
+    return LGF_OK;
 }
 
 int lgf_last_flow_seconds(lgf_lattice* lat, double* seconds) {
@@ -908,7 +942,10 @@ int lgf_debug_fields(lgf_lattice* lat, double* clover_F, double* improved_F) {
     double2 *dc = nullptr, *di = nullptr;
     LGF_CUDA_TRY(ctx, cudaMalloc(&dc, bytes));
     cudaError_t e = cudaMalloc(&di, bytes);
-    int rc = e == cudaSuccess ? single_measure(ctx, b, nullptr, nullptr, dc, di)
+    MeasOut mo{};
+    mo.dbg_clover = dc;
+    mo.dbg_improved = di;
+    int rc = e == cudaSuccess ? single_measure(ctx, b, mo)
                               : set_error(ctx, LGF_ENOMEM, "debug field buffers: %s", cudaGetErrorString(e));
     if (rc == LGF_OK && clover_F) e = cudaMemcpy(clover_F, dc, bytes, cudaMemcpyDeviceToHost);
     if (rc == LGF_OK && e == cudaSuccess && improved_F) e = cudaMemcpy(improved_F, di, bytes, cudaMemcpyDeviceToHost);

@@ -284,22 +284,37 @@ constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
 // Shared memory of one measurement block: the straight lines of length 2 and
 // 3 from each of its 32 sites in the 8 signed directions (every plane and
 // quadrant of the site reuses them), then the per-plane results.
-template <typename R> struct MeasSmem {
-    R line[8][2][18][MEAS_SITES];  // [2*dir + (sign<0)][length-2][entry][site]
-    alg<R> F[6][MEAS_SITES];
+template <typename R, bool OUT> struct MeasSmem {
+    R line[8][2][18][MEAS_SITES];     // [2*dir + (sign<0)][length-2][entry][site]
+    alg<R> F[6][MEAS_SITES];          // improved F per plane
+    alg<R> C[OUT ? 6 : 1][MEAS_SITES];  // clover F per plane (single-lattice passes only)
     double E[6][MEAS_SITES];
 };
 
-template <typename R>
-__device__ __forceinline__ void store_line(MeasSmem<R>* sm, int sdir, int len, int lane, const su3<R>& L) {
+// Optional per-site / per-(site, plane) outputs of a measurement pass (all
+// null in the flow).  e, q: the densities of E and Q; e_imp, q_clov: the
+// energy density with the improved F (ImprovedEnergyDensity.cpp:13-20) and
+// the charge density with the clover F (UnImprovedTopologicalCharge.cpp:11-16);
+// dbg_*: F and F^ as Hermitian 3x3 matrices per (site, plane).
+struct MeasOut {
+    double* e;
+    double* q;
+    double* e_imp;
+    double* q_clov;
+    double2* dbg_clover;
+    double2* dbg_improved;
+};
+
+template <typename R, bool OUT>
+__device__ __forceinline__ void store_line(MeasSmem<R, OUT>* sm, int sdir, int len, int lane, const su3<R>& L) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
         sm->line[sdir][len - 2][2 * k][lane] = L.m[k].re;
         sm->line[sdir][len - 2][2 * k + 1][lane] = L.m[k].im;
     }
 }
-template <typename R>
-__device__ __forceinline__ su3<R> load_line(const MeasSmem<R>* sm, int sdir, int len, int lane) {
+template <typename R, bool OUT>
+__device__ __forceinline__ su3<R> load_line(const MeasSmem<R, OUT>* sm, int sdir, int len, int lane) {
     su3<R> L;
 #pragma unroll
     for (int k = 0; k < 9; ++k) L.m[k] = cmk<R>(sm->line[sdir][len - 2][2 * k][lane], sm->line[sdir][len - 2][2 * k + 1][lane]);
@@ -309,9 +324,9 @@ __device__ __forceinline__ su3<R> load_line(const MeasSmem<R>* sm, int sdir, int
 // Clover F and improved F of plane (mu, nu) at the thread's site, using the
 // block's shared lines (21 matrix products and 16 global link loads per
 // quadrant).  See the comment above Plane for the leaf decomposition.
-template <typename R>
+template <typename R, bool OUT>
 __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
-                                                  int mu, int nu, const MeasSmem<R>* sm, int lane, alg<R>& F11,
+                                                  int mu, int nu, const MeasSmem<R, OUT>* sm, int lane, alg<R>& F11,
                                                   alg<R>& Fhat) {
     Plane<R> P;
     P.U = U;
@@ -405,23 +420,20 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
 // lines of signed direction w, and w+6 for w < 2) into shared memory.  Phase
 // 1: F and F^ of every (site, plane).  Phase 2: the six planes meet in shared
 // memory for e(x) and q(x); the tile's sums go to the lattice's
-// partial[slice * nchunk + chunk] (double2).  site_e/site_q (single-lattice
-// use) receive e(x), q(x) per site; dbg_clover/dbg_improved receive F and F^
-// per (site, plane) as Hermitian 3x3 matrices (parity tests).
+// partial[slice * nchunk + chunk] (double2).  The optional outputs of
+// MeasOut (single-lattice passes) receive per-site densities and per
+// (site, plane) F and F^.
 //   e(x) = sum_{mu<nu} ReTr(F F)                 (EnergyDensity.cpp:13-20)
 //   q(x) = ReTr(F^32 F^01) + ReTr(F^31 F^20) + ReTr(F^30 F^12)
 //        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
 //                                             (TopologicalCharge.cpp:11-16)
-template <typename R>
+template <typename R, bool OUT = false>
 __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const LatDesc<R>* __restrict__ descs,
                                                                            const int4* __restrict__ mtiles,
                                                                            const int* __restrict__ nmtiles,
-                                                                           double* __restrict__ site_e,
-                                                                           double* __restrict__ site_q,
-                                                                           double2* __restrict__ dbg_clover,
-                                                                           double2* __restrict__ dbg_improved) {
+                                                                           MeasOut out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MeasSmem<R>* sm = reinterpret_cast<MeasSmem<R>*>(smem_raw);
+    MeasSmem<R, OUT>* sm = reinterpret_cast<MeasSmem<R, OUT>*>(smem_raw);
     const int lane = threadIdx.x, p = threadIdx.y;
     const int n = *nmtiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
@@ -455,12 +467,13 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const
         // phase 1: this thread's plane
         if (valid) {
             alg<R> F11, Fh;
-            plane_fields_smem<R>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, F11, Fh);
+            plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, F11, Fh);
             sm->F[p][lane] = Fh;
             sm->E[p][lane] = retr_hh(F11, F11);
-            if (dbg_clover) {
-                store_alg_as_herm(dbg_clover + ((size_t)s * 6 + p) * 9, F11);
-                store_alg_as_herm(dbg_improved + ((size_t)s * 6 + p) * 9, Fh);
+            if (OUT) {
+                sm->C[p][lane] = F11;
+                if (out.dbg_clover) store_alg_as_herm(out.dbg_clover + ((size_t)s * 6 + p) * 9, F11);
+                if (out.dbg_improved) store_alg_as_herm(out.dbg_improved + ((size_t)s * 6 + p) * 9, Fh);
             }
         }
         __syncthreads();
@@ -472,8 +485,17 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const
                     (sm->E[4][lane] + sm->E[5][lane]);
                 q = -retr_hh(sm->F[5][lane], sm->F[0][lane]) + retr_hh(sm->F[4][lane], sm->F[1][lane]) -
                     retr_hh(sm->F[2][lane], sm->F[3][lane]);
-                if (site_e) site_e[s] = e;
-                if (site_q) site_q[s] = q;
+                if (OUT && out.e) out.e[s] = e;
+                if (OUT && out.q) out.q[s] = q;
+                if (OUT && out.e_imp) {
+                    double ei = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) ei += retr_hh(sm->F[k][lane], sm->F[k][lane]);
+                    out.e_imp[s] = ei;
+                }
+                if (OUT && out.q_clov)
+                    out.q_clov[s] = -retr_hh(sm->C[5][lane], sm->C[0][lane]) + retr_hh(sm->C[4][lane], sm->C[1][lane]) -
+                                    retr_hh(sm->C[2][lane], sm->C[3][lane]);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -488,9 +510,10 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const
 
 // Dynamic shared memory of k_measure<R> (above 48 KB for double: the
 // attribute must be raised once per device before the first launch).
-template <typename R> inline size_t measure_smem_bytes() { return sizeof(MeasSmem<R>); }
-template <typename R> inline cudaError_t prepare_measure_kernel() {
-    return cudaFuncSetAttribute(k_measure<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MeasSmem<R>));
+template <typename R, bool OUT = false> inline size_t measure_smem_bytes() { return sizeof(MeasSmem<R, OUT>); }
+template <typename R, bool OUT = false> inline cudaError_t prepare_measure_kernel() {
+    return cudaFuncSetAttribute(k_measure<R, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(MeasSmem<R, OUT>));
 }
 
 constexpr int RED_THREADS = 256;

@@ -328,6 +328,50 @@ void MeasureQdensityDistribution(SimulationParameters& params, FlowParameters& f
     qdensity_impl(params, flowParams);
 }
 
+// MeasureFlowedGaugeConfigurations (LGF.cpp:228-255): the clover-F charge and
+// the improved-F energy density of each flowed configuration, one CSV row each.
+static int measure_flowed_impl(SimulationParameters& params, FlowParameters& fp) {
+    if (!check_params(params)) return LGF_EINVAL;
+    int rc = LGF_OK;
+    lgf_ctx* ctx = nullptr;
+    const int shape[4] = {params.getshape(0), params.getshape(1), params.getshape(2), params.getshape(3)};
+    const long long V = 1LL * shape[0] * shape[1] * shape[2] * shape[3];
+    const double pickup = fp.getepsilon() * fp.getflowSteps();  // LGF.cpp:231
+    int status = LGF_OK;
+    for (int i = fp.getConfigurationStart(); i <= fp.getConfigurationStop(); i++) {
+        std::vector<double> links((size_t)V * 4 * 18);
+        const std::string ensembleNum = std::to_string(i);
+        if (!load_links(params, "GF", fp.getdataFolder(), ensembleNum + "_Flowtime" + std::to_string(pickup), links)) {
+            status = LGF_EIO;
+            continue;
+        }
+        if (!ctx && !(ctx = context(&rc))) return rc;
+        lgf_lattice* lat = nullptr;
+        double Eimp = 0.0, Qclov = 0.0;
+        rc = lgf_lattice_create(ctx, shape, g_state.precision, &lat);
+        if (rc == LGF_OK) rc = lgf_upload_links(lat, links.data());
+        if (rc == LGF_OK) rc = lgf_measure_flowed(lat, &Eimp, &Qclov);
+        if (lat) lgf_lattice_destroy(lat);
+        if (rc != LGF_OK) {
+            std::cout << "LGF engine: " << lgf_last_error(ctx) << "\n";
+            status = rc;
+            continue;
+        }
+        std::cout << "Topological Charge = " << Qclov << "\n";
+        std::cout.flush();
+        std::cout << "Energy Density\t   = " << Eimp << "\n";
+        std::cout.flush();
+        const std::vector<double> t{pickup};
+        append_csv(params, "UnImprovedTopological_Charge", "GF", fp.getdataFolder(), "_" + ensembleNum, t, {Qclov});
+        append_csv(params, "ImprovedEnergyDensity", "GF", fp.getdataFolder(), "_" + ensembleNum, t, {Eimp});
+    }
+    return status;
+}
+
+void MeasureFlowedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams) {
+    measure_flowed_impl(params, flowParams);
+}
+
 extern "C" {
 
 int lgf_dropin_configure(int precision, int reunit_every, int device) {
@@ -357,6 +401,14 @@ int lgf_dropin_resume_flowed(const int shape[4], double beta, int config_start, 
     SimulationParameters p(4, 4, {shape[0], shape[1], shape[2], shape[3]}, beta, {0, 0, 0, 0}, "torus");
     FlowParameters f(config_start, config_stop, flow_steps, epsilon, measure_every, data_folder);
     return resume_impl(p, f, flow_time_pickup);
+}
+
+int lgf_dropin_measure_flowed(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
+                              double epsilon, int measure_every, const char* data_folder) {
+    if (!shape || !data_folder) return LGF_EINVAL;
+    SimulationParameters p(4, 4, {shape[0], shape[1], shape[2], shape[3]}, beta, {0, 0, 0, 0}, "torus");
+    FlowParameters f(config_start, config_stop, flow_steps, epsilon, measure_every, data_folder);
+    return measure_flowed_impl(p, f);
 }
 
 int lgf_dropin_measure_qdensity(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,

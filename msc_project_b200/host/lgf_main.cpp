@@ -3,7 +3,7 @@
 //
 //   lgf_flow NrDims extdofs beta shape[NrDims] cuts[NrDims] configStart configStop
 //            flowSteps epsilon measureInterval dataFolder
-//            [--workflow flow|resume=<t>|qdensity] [--precision fp64|fp32mixed]
+//            [--workflow flow|resume=<t>|qdensity|measure] [--precision fp64|fp32mixed]
 //            [--reunit-every k] [--device d]
 //
 // cuts are accepted and ignored (one GPU holds the whole lattice).  The
@@ -68,6 +68,8 @@ int main(int argc, char** argv) {
         ResumeFlowedConfiguration(params, flowParams, std::stod(workflow.substr(7)));
     } else if (workflow == "qdensity") {
         MeasureQdensityDistribution(params, flowParams);
+    } else if (workflow == "measure") {
+        MeasureFlowedGaugeConfigurations(params, flowParams);
     } else {
         std::cerr << "lgf_flow: unknown workflow " << workflow << "\n";
         return 2;

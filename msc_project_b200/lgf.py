@@ -4,7 +4,8 @@ The names follow the LGF reference so tests read like its own workflow:
 ``SimulationParameters`` / ``FlowParameters`` (LGF/SimulationParameters.h),
 ``FlowSavedGaugeConfigurations`` (LGF/LGF.cpp:163-196),
 ``ResumeFlowedConfiguration`` (LGF/LGF.cpp:197-226),
-``MeasureQdensityDistribution`` (LGF/LGF.cpp:114-124) -- these three call the
+``MeasureQdensityDistribution`` (LGF/LGF.cpp:114-124),
+``MeasureFlowedGaugeConfigurations`` (LGF/LGF.cpp:228-255) -- these four call the
 C++ drop-in inside liblgf_b200.so -- plus ``Context`` / ``Lattice`` for direct
 use of the engine (upload, flow, measure, batch, serve).
 
@@ -186,6 +187,13 @@ class Lattice:
         self.ctx.check(self.lib.lgf_site_densities(self.h, _dp(e), _dp(q)))
         return e, q
 
+    def measure_flowed(self):
+        """(E with the improved F, Q with the clover F): MeasureFlowedGaugeConfigurations' observables."""
+        a = ctypes.c_double()
+        b = ctypes.c_double()
+        self.ctx.check(self.lib.lgf_measure_flowed(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def unitarity(self):
         a = ctypes.c_double()
         b = ctypes.c_double()
@@ -341,6 +349,13 @@ def ResumeFlowedConfiguration(params, flowParams, flowTime_pickup: float) -> int
     return lib.lgf_dropin_resume_flowed(_shape(params.shape), params.beta, flowParams.start, flowParams.stop,
                                         flowParams.flowSteps, flowParams.epsilon, flowParams.measureEvery,
                                         flowParams.dataFolder.encode(), flowTime_pickup)
+
+
+def MeasureFlowedGaugeConfigurations(params, flowParams) -> int:
+    lib = C.load()
+    return lib.lgf_dropin_measure_flowed(_shape(params.shape), params.beta, flowParams.start, flowParams.stop,
+                                         flowParams.flowSteps, flowParams.epsilon, flowParams.measureEvery,
+                                         flowParams.dataFolder.encode())
 
 
 def MeasureQdensityDistribution(params, flowParams) -> int:

@@ -150,6 +150,10 @@ def test_dropin_flow_saved_matches_reference_outputs(ctx, tmp_path):
     csv_e = (obs / "EnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text()
     assert csv_q == g["csv_topcharge"]
     assert csv_e == g["csv_energy"]
+    import pandas as pd
+    df = pd.read_csv(obs / "EnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv", index_col="t",
+                     names=["t", "E0"], sep=",", header=None)
+    assert len(df) == 101 and df.index[0] == 0.0 and abs(df.index[-1] - 1.0) < 1e-12
     flowed = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/GF" / g["flowed_file"]
     Uf = np.fromfile(flowed)
     assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < TOL
@@ -189,7 +193,59 @@ def test_qdensity_output(ctx, tmp_path):
     q = np.fromfile(tmp_path / "Observables/Qdensity/beta6_000000/8X8X8X8/GF/torus_extdof1_0_Flowtime1.000000.bin")
     _, qo = O.site_densities(U, (8, 8, 8, 8))
     assert q.shape == (8 ** 4,)
+    assert np.reshape(q[: 8 * 8], (8, 8)).shape == (8, 8)  # the analysis slices x-y planes of this array
     assert np.max(np.abs(q - (np.pi ** 2 / 4) * qo)) < 1e-11  # the reference's pi^2/4 prefactor
+
+
+def _retr(a, b):
+    A = (a[0::2] + 1j * a[1::2]).reshape(3, 3)
+    B = (b[0::2] + 1j * b[1::2]).reshape(3, 3)
+    return float(np.trace(A @ B).real)
+
+
+def test_measure_flowed_observables_against_oracle(ctx):
+    """ImprovedEnergyDensity (improved F) and UnImprovedTopologicalCharge (clover F)."""
+    shape = (4, 4, 6, 6)
+    U = golden_links("g4466_seed7.bin")
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        Ei, Qc = lat.measure_flowed()
+    planes = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
+    V = O.volume(shape)
+    se = sq = 0.0
+    for x in range(V):
+        Fh = [O.improved_F(U, shape, x, a, b) for a, b in planes]
+        Fc = [O.clover_F(U, shape, x, a, b) for a, b in planes]
+        se += sum(_retr(f, f) for f in Fh)
+        sq += -_retr(Fc[5], Fc[0]) + _retr(Fc[4], Fc[1]) - _retr(Fc[2], Fc[3])
+    assert abs(Ei - se / V) < 1e-12 * abs(se / V)
+    assert abs(Qc - sq / (4 * np.pi ** 2)) < 1e-12
+
+
+def test_dropin_measure_flowed_outputs_read_like_the_analysis(ctx, tmp_path):
+    import pandas as pd
+    from msc_project_b200 import FlowParameters, MeasureFlowedGaugeConfigurations, SimulationParameters, configure
+    configure(FP64)
+    shape = [4, 4, 6, 6]
+    gf = tmp_path / "ensembles/su3/beta6_000000/4X4X6X6/GF"
+    gf.mkdir(parents=True)
+    U = golden_links("g4466_seed7.bin")
+    U.tofile(gf / "torus_extdof4_0_Flowtime1.000000.bin")
+    rc = MeasureFlowedGaugeConfigurations(SimulationParameters(4, 4, shape, 6.0, [0, 0, 0, 0]),
+                                          FlowParameters(0, 0, 100, 0.01, 1, str(tmp_path) + "/"))
+    assert rc == 0
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        Ei, Qc = lat.measure_flowed()
+    obs = tmp_path / "Observables"
+    # read the way the offline analysis reads its CSVs (t as the index, one column per configuration)
+    q = pd.read_csv(obs / "UnImprovedTopological_Charge/beta6_000000/4X4X6X6/GF/torus_extdof4_0.csv",
+                    index_col="t", names=["t", "Q0"], sep=",", header=None)
+    e = pd.read_csv(obs / "ImprovedEnergyDensity/beta6_000000/4X4X6X6/GF/torus_extdof4_0.csv",
+                    index_col="t", names=["t", "E0"], sep=",", header=None)
+    assert list(q.index) == [1.0] and list(e.index) == [1.0]
+    assert abs(q["Q0"].iloc[0] - Qc) <= 5e-6 * max(1.0, abs(Qc))
+    assert abs(e["E0"].iloc[0] - Ei) <= 5e-6 * abs(Ei)
 
 
 # ------------------------------------------------------------- properties
