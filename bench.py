@@ -329,6 +329,24 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
             "all_done": all(s.state == 2 for s in sts)}
 
 
+def form_heatbath(ctx):
+    """Input generation: hot start and 20 x (Cabibbo-Marinari heatbath + 5
+    overrelaxation sweeps) at beta = 6.0 on 24^3x48, FP64.  Rate in
+    site-sweeps/s (one sweep = every link updated once, HB or OR)."""
+    import numpy as np
+    from msc_project_b200 import FP64
+    V = int(np.prod(SHAPE))
+    with ctx.lattice(SHAPE, FP64) as lat:
+        lat.hot_start(1)
+        lat.heatbath(6.0, 1, 5, seed=1)  # warm-up
+        t0 = time.perf_counter()
+        rej = lat.heatbath(6.0, 20, 5, seed=2)
+        sec = time.perf_counter() - t0
+        plaq = lat.plaquette()
+    return {"config": "24^3x48, beta 6.0, 20 x (CM heatbath + 5 OR)", "site_sweeps_per_s": V * 20 * 6 / sec,
+            "seconds": sec, "plaquette": plaq, "rejected_subgroup_updates": rej}
+
+
 # ------------------------------------------------------------------ engine
 def engine_arm(args):
     import numpy as np
@@ -407,7 +425,7 @@ def engine_arm(args):
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = {"fp32mixed": form_fp32mixed(ctx), "batched": form_batched(ctx),
-                 "served": form_served(ctx, args.serve_jobs, args.serve_rate)}
+                 "served": form_served(ctx, args.serve_jobs, args.serve_rate), "heatbath": form_heatbath(ctx)}
 
     launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
     line = {

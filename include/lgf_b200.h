@@ -151,6 +151,23 @@ int lgf_last_flow_seconds(lgf_lattice* lat, double* seconds);
  * streams, other host threads) race and must be ordered by the caller. */
 int lgf_measure_noalloc(const double* links, const int shape[4], double* out, void* stream);
 
+/* ------------------------------------------------------- configurations */
+/* Input generation on the GPU (SU3_field::InitializeHotStart / ColdStart,
+ * LGF/Field/SU3_field.cpp:440-466; SU3_Heatbath::update,
+ * LGF/SU3_Heatbath/SU3_Heatbath.cpp:16-224).  lgf_heatbath runs n_iter x (one
+ * Cabibbo-Marinari heatbath sweep + or_per_hb overrelaxation sweeps) at beta,
+ * drawing from a counter-based generator keyed by seed; successive calls on
+ * the same lattice continue the stream.  *rejected (may be NULL) counts SU(2)
+ * subgroup updates whose bounded rejection loop found no sample (left unchanged). */
+int lgf_hot_start(lgf_lattice* lat, uint64_t seed);
+int lgf_cold_start(lgf_lattice* lat);
+int lgf_heatbath(lgf_lattice* lat, double beta, int n_iter, int or_per_hb, uint64_t seed, uint64_t* rejected);
+/* n_sweeps overrelaxation sweeps alone (SU3_Heatbath::OverRelaxation, SU3_Heatbath.cpp:58-111):
+ * microcanonical, the Wilson action is unchanged up to rounding */
+int lgf_overrelax(lgf_lattice* lat, int n_sweeps);
+/* SU3_field::Avg_Plaquette (SU3_field.cpp:485-499): sum ReTr P / (3 * 6 * V) */
+int lgf_plaquette(lgf_lattice* lat, double* avg);
+
 /* ------------------------------------------------------------------ batch */
 /* A flow job: one configuration, its flow schedule and its result arrays. */
 typedef struct lgf_job {

@@ -14,6 +14,10 @@
  *       (LGF/LGF.h:35, LGF/LGF.cpp:114-124)
  *   void MeasureFlowedGaugeConfigurations(SimulationParameters&, FlowParameters&)
  *       (LGF/LGF.h:34, LGF/LGF.cpp:228-255)
+ *   HBParameters(start, stop, ThermSteps, OR_per_HB, configSep, dataFolder)
+ *       (LGF/SimulationParameters.h:88-124) and
+ *   void GenerateHeatBathGaugeConfigurations(SimulationParameters&, HBParameters&)
+ *       (LGF/LGF.h:29, LGF/LGF.cpp:136-160), the input generator
  * with the same input/output files (ensembles/.../*.bin, Observables/.../*.csv)
  * and the same stdout lines; the flow and the measurements run on the GPU
  * through lgf_b200.h.  Other languages bind the extern "C" functions at the end.
@@ -24,6 +28,8 @@
  */
 #ifndef LGF_DROPIN_H
 #define LGF_DROPIN_H
+
+#include <stdint.h>
 
 #ifdef __cplusplus
 #include <string>
@@ -74,7 +80,33 @@ private:
     std::string m_dataFolder;
 };
 
+class HBParameters {
+public:
+    HBParameters(int ConfigurationStart, int ConfigurationStop, int ThermSteps, int OR_per_HB, int configSep,
+                 const std::string& dataFolder)
+        : m_ConfigurationStart(ConfigurationStart), m_ConfigurationStop(ConfigurationStop), m_ThermSteps(ThermSteps),
+          m_OR_per_HB(OR_per_HB), m_configSep(configSep), m_dataFolder(dataFolder) {}
+    int getConfigurationStart() { return m_ConfigurationStart; }
+    int getConfigurationStop() { return m_ConfigurationStop; }
+    int getThermSteps() { return m_ThermSteps; }
+    int getOR_per_HB() { return m_OR_per_HB; }
+    int getconfigSep() { return m_configSep; }
+    std::string getdataFolder() { return m_dataFolder; }
+
+private:
+    int m_ConfigurationStart;
+    int m_ConfigurationStop;
+    int m_ThermSteps;
+    int m_OR_per_HB;
+    int m_configSep;
+    std::string m_dataFolder;
+};
+
 void FlowSavedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams);
+/* GenerateHeatBathGaugeConfigurations (LGF/LGF.cpp:136-160) on the GPU; the
+ * generator seed comes from LGF_SEED in the environment, else std::random_device
+ * (the reference's default, LGF/Math/Random.h:18-22). */
+void GenerateHeatBathGaugeConfigurations(SimulationParameters& params, HBParameters& HBparams);
 void ResumeFlowedConfiguration(SimulationParameters& params, FlowParameters& flowParams, double flowTime_pickup);
 void MeasureQdensityDistribution(SimulationParameters& params, FlowParameters& flowParams);
 void MeasureFlowedGaugeConfigurations(SimulationParameters& params, FlowParameters& flowParams);
@@ -97,6 +129,8 @@ int lgf_dropin_measure_qdensity(const int shape[4], double beta, int config_star
                                 double epsilon, int measure_every, const char* data_folder);
 int lgf_dropin_measure_flowed(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,
                               double epsilon, int measure_every, const char* data_folder);
+int lgf_dropin_generate_heatbath(const int shape[4], double beta, int config_start, int config_stop, int therm_steps,
+                                 int or_per_hb, int config_sep, const char* data_folder, uint64_t seed);
 
 #ifdef __cplusplus
 }

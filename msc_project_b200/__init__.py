@@ -7,5 +7,6 @@ Python mirror for tests and benchmarks.
 """
 from ._capi import LIB_PATH, load  # noqa: F401
 from .lgf import (FP32MIXED, FP64, Context, FlowParameters, FlowResult, FlowSavedGaugeConfigurations,  # noqa: F401
+                  GenerateHeatBathGaugeConfigurations, HBParameters,
                   Job, Lattice, LGFError, MeasureFlowedGaugeConfigurations, MeasureQdensityDistribution, ResumeFlowedConfiguration, Server,
                   SimulationParameters, configure, volume)

@@ -83,6 +83,12 @@ SIGNATURES = {
     "lgf_profile_kernels": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _dp]),
     "lgf_last_flow_seconds": (ctypes.c_int, [_vp, _dp]),
     "lgf_measure_noalloc": (ctypes.c_int, [_dp, _ip, _dp, _vp]),
+    "lgf_hot_start": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "lgf_cold_start": (ctypes.c_int, [_vp]),
+    "lgf_heatbath": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                    ctypes.POINTER(ctypes.c_uint64)]),
+    "lgf_plaquette": (ctypes.c_int, [_vp, _dp]),
+    "lgf_overrelax": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lgf_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_job), ctypes.c_int, ctypes.POINTER(lgf_batch_stats)]),
     "lgf_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip]),
     "lgf_serve_start": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_serve_config), ctypes.POINTER(_vp)]),
@@ -97,6 +103,8 @@ SIGNATURES = {
                                                 ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_double]),
     "lgf_dropin_measure_flowed": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
+    "lgf_dropin_generate_heatbath": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_uint64]),
     "lgf_dropin_measure_qdensity": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
 }

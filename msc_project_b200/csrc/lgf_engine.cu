@@ -509,13 +509,6 @@ int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host) {
 
 using namespace lgf;
 
-struct lgf_lattice {
-    lgf_ctx* ctx = nullptr;
-    LatticeBuf buf;
-    GroupBase* group = nullptr;  // single-member group, created on first flow
-    int group_threads = 0;
-    double last_flow_s = 0.0;
-};
 
 // One measurement-kernel pass over a single lattice with per-site (and,
 // when asked, per (site, plane) F / F^) outputs; no reduction.

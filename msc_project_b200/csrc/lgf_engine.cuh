@@ -89,3 +89,12 @@ int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host);
 int count_measurements(const lgf_flow_opts& o);
 
 }  // namespace lgf
+
+struct lgf_lattice {
+    lgf_ctx* ctx = nullptr;
+    lgf::LatticeBuf buf;
+    lgf::GroupBase* group = nullptr;  // single-member group, created on first flow
+    int group_threads = 0;
+    double last_flow_s = 0.0;
+    unsigned long long hb_epoch = 0;  // heatbath random-number stream position
+};

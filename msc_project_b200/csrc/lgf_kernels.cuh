@@ -43,8 +43,7 @@ namespace lgf {
 // A = sum_{nu != mu} U_nu(x+mu) (U_nu(x) U_mu(x+nu))^dag
 //                  + (U_mu(x-nu) U_nu(x-nu+mu))^dag U_nu(x-nu)
 template <typename R>
-__device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
-                                                int mu, su3<R>& u_out) {
+__device__ __forceinline__ su3<R> staple_sum(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c, int mu) {
     const int V = g.V;
     const Dir dm = dir_of(g, c, mu);
     su3<R> S;
@@ -71,8 +70,15 @@ __device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, c
             acc_an(S, t, b3);
         }
     }
-    u_out = load_link(U, V, mu, s);
-    su3<R> W = mul_nn(u_out, S);
+    return S;
+}
+
+template <typename R>
+__device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                                int mu, su3<R>& u_out) {
+    const su3<R> S = staple_sum<R>(U, g, s, c, mu);
+    u_out = load_link(U, g.V, mu, s);
+    const su3<R> W = mul_nn(u_out, S);
     return ta_part(W, R(-0.5));
 }
 

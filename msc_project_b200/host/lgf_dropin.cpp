@@ -16,6 +16,7 @@
 #include <filesystem>
 #include <fstream>
 #include <iostream>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -372,6 +373,68 @@ void MeasureFlowedGaugeConfigurations(SimulationParameters& params, FlowParamete
     measure_flowed_impl(params, flowParams);
 }
 
+// GenerateHeatBathGaugeConfigurations (LGF.cpp:136-160): hot start and
+// thermalisation for a new ensemble (ThermSteps != 0 and start == 0), else
+// continue from the saved configuration `start`; then one saved configuration
+// every configSep updates.  update(n) prints "step: i" per iteration like
+// SU3_Heatbath::update (SU3_Heatbath.cpp:16-25).
+static int heatbath_impl(SimulationParameters& params, HBParameters& hb, uint64_t seed) {
+    if (!check_params(params)) return LGF_EINVAL;
+    int rc = LGF_OK;
+    lgf_ctx* ctx = context(&rc);
+    if (!ctx) return rc;
+    const int shape[4] = {params.getshape(0), params.getshape(1), params.getshape(2), params.getshape(3)};
+    const long long V = 1LL * shape[0] * shape[1] * shape[2] * shape[3];
+    const std::string method = "Heatbath_" + std::to_string(hb.getOR_per_HB()) + "_ORperHB";  // SU3_Heatbath.cpp:6
+    lgf_lattice* lat = nullptr;
+    rc = lgf_lattice_create(ctx, shape, g_state.precision, &lat);
+    if (rc != LGF_OK) {
+        std::cout << "LGF engine: " << lgf_last_error(ctx) << "\n";
+        return rc;
+    }
+    std::vector<double> links((size_t)V * 4 * 18);
+    const bool fresh = hb.getThermSteps() != 0 && hb.getConfigurationStart() == 0;
+    if (fresh) {
+        rc = lgf_hot_start(lat, seed);
+    } else if (!load_links(params, method, hb.getdataFolder(), std::to_string(hb.getConfigurationStart()), links)) {
+        rc = LGF_EIO;
+    } else {
+        rc = lgf_upload_links(lat, links.data());
+    }
+    auto update = [&](int n) {
+        for (int i = 0; i < n && rc == LGF_OK; ++i) {
+            rc = lgf_heatbath(lat, params.getbeta(), 1, hb.getOR_per_HB(), seed, nullptr);
+            std::cout << "step: " << i << std::endl;
+        }
+    };
+    auto save = [&](int cfg) {
+        if (rc == LGF_OK) rc = lgf_download_links(lat, links.data());
+        if (rc == LGF_OK && !save_links(params, method, hb.getdataFolder(), std::to_string(cfg), links)) rc = LGF_EIO;
+    };
+    if (fresh) {
+        update(hb.getThermSteps());
+        save(hb.getConfigurationStart());
+    }
+    for (int i = hb.getConfigurationStart() + 1; i <= hb.getConfigurationStop() && rc == LGF_OK; i++) {
+        update(hb.getconfigSep());
+        save(i);
+    }
+    if (rc != LGF_OK && rc != LGF_EIO) std::cout << "LGF engine: " << lgf_last_error(ctx) << "\n";
+    lgf_lattice_destroy(lat);
+    return rc;
+}
+
+static uint64_t env_seed() {
+    const char* s = std::getenv("LGF_SEED");
+    if (s) return std::strtoull(s, nullptr, 10);
+    std::random_device rd;
+    return ((uint64_t)rd() << 32) ^ rd();
+}
+
+void GenerateHeatBathGaugeConfigurations(SimulationParameters& params, HBParameters& HBparams) {
+    heatbath_impl(params, HBparams, env_seed());
+}
+
 extern "C" {
 
 int lgf_dropin_configure(int precision, int reunit_every, int device) {
@@ -409,6 +472,14 @@ int lgf_dropin_measure_flowed(const int shape[4], double beta, int config_start,
     SimulationParameters p(4, 4, {shape[0], shape[1], shape[2], shape[3]}, beta, {0, 0, 0, 0}, "torus");
     FlowParameters f(config_start, config_stop, flow_steps, epsilon, measure_every, data_folder);
     return measure_flowed_impl(p, f);
+}
+
+int lgf_dropin_generate_heatbath(const int shape[4], double beta, int config_start, int config_stop, int therm_steps,
+                                 int or_per_hb, int config_sep, const char* data_folder, uint64_t seed) {
+    if (!shape || !data_folder || therm_steps < 0 || or_per_hb < 0 || config_sep < 0) return LGF_EINVAL;
+    SimulationParameters p(4, 4, {shape[0], shape[1], shape[2], shape[3]}, beta, {0, 0, 0, 0}, "torus");
+    HBParameters h(config_start, config_stop, therm_steps, or_per_hb, config_sep, data_folder);
+    return heatbath_impl(p, h, seed);
 }
 
 int lgf_dropin_measure_qdensity(const int shape[4], double beta, int config_start, int config_stop, int flow_steps,

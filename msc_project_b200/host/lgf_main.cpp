@@ -7,7 +7,10 @@
 //            [--reunit-every k] [--device d]
 //
 // cuts are accepted and ignored (one GPU holds the whole lattice).  The
-// workflow defaults to FlowSavedGaugeConfigurations.
+// workflow defaults to FlowSavedGaugeConfigurations; an integer in the epsilon
+// position selects GenerateHeatBathGaugeConfigurations with ThermSteps =
+// flowSteps, OR_per_HB = that integer and configSep = measureInterval, as in
+// the reference's ParseCLargs.
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -52,9 +55,15 @@ int main(int argc, char** argv) {
     const int start = std::stoi(pos[i++]);
     const int stop = std::stoi(pos[i++]);
     const int steps = std::stoi(pos[i++]);
-    const double eps = std::stod(pos[i++]);
+    // an integer in the epsilon position selects the heatbath (ParseCLargs, LGF.cpp:326-335)
+    const std::string eps_arg = pos[i++];
+    size_t used = 0;
+    std::stoi(eps_arg, &used);
+    const bool heatbath = used == eps_arg.size();
+    const double eps = heatbath ? 0.0 : std::stod(eps_arg);
     const int interval = std::stoi(pos[i++]);
     const std::string folder = pos[i++];
+    if (heatbath && workflow == "flow") workflow = "heatbath";
     std::cout << "Started Parallel Session with 1 processes...\n";
     if (lgf_dropin_configure(precision, reunit, device) != LGF_OK) {
         std::cerr << "lgf_flow: bad engine options\n";
@@ -62,7 +71,10 @@ int main(int argc, char** argv) {
     }
     SimulationParameters params(NrDims, extdofs, shape, beta, cuts, "torus");
     FlowParameters flowParams(start, stop, steps, eps, interval, folder);
-    if (workflow == "flow") {
+    if (workflow == "heatbath") {
+        HBParameters hb(start, stop, steps, std::stoi(eps_arg), interval, folder);
+        GenerateHeatBathGaugeConfigurations(params, hb);
+    } else if (workflow == "flow") {
         FlowSavedGaugeConfigurations(params, flowParams);
     } else if (workflow.rfind("resume=", 0) == 0) {
         ResumeFlowedConfiguration(params, flowParams, std::stod(workflow.substr(7)));

@@ -187,6 +187,27 @@ class Lattice:
         self.ctx.check(self.lib.lgf_site_densities(self.h, _dp(e), _dp(q)))
         return e, q
 
+    def hot_start(self, seed: int):
+        self.ctx.check(self.lib.lgf_hot_start(self.h, ctypes.c_uint64(seed)))
+
+    def cold_start(self):
+        self.ctx.check(self.lib.lgf_cold_start(self.h))
+
+    def heatbath(self, beta: float, n_iter: int, or_per_hb: int, seed: int) -> int:
+        """n_iter x (heatbath sweep + or_per_hb overrelaxation sweeps); returns rejected subgroup updates."""
+        rej = ctypes.c_uint64()
+        self.ctx.check(self.lib.lgf_heatbath(self.h, beta, n_iter, or_per_hb, ctypes.c_uint64(seed),
+                                             ctypes.byref(rej)))
+        return rej.value
+
+    def overrelax(self, n_sweeps: int):
+        self.ctx.check(self.lib.lgf_overrelax(self.h, n_sweeps))
+
+    def plaquette(self) -> float:
+        p = ctypes.c_double()
+        self.ctx.check(self.lib.lgf_plaquette(self.h, ctypes.byref(p)))
+        return p.value
+
     def measure_flowed(self):
         """(E with the improved F, Q with the clover F): MeasureFlowedGaugeConfigurations' observables."""
         a = ctypes.c_double()
@@ -349,6 +370,21 @@ def ResumeFlowedConfiguration(params, flowParams, flowTime_pickup: float) -> int
     return lib.lgf_dropin_resume_flowed(_shape(params.shape), params.beta, flowParams.start, flowParams.stop,
                                         flowParams.flowSteps, flowParams.epsilon, flowParams.measureEvery,
                                         flowParams.dataFolder.encode(), flowTime_pickup)
+
+
+class HBParameters:
+    """LGF/SimulationParameters.h:88-124 (same constructor arguments)."""
+
+    def __init__(self, ConfigurationStart, ConfigurationStop, ThermSteps, OR_per_HB, configSep, dataFolder):
+        self.start, self.stop, self.ThermSteps = ConfigurationStart, ConfigurationStop, ThermSteps
+        self.OR_per_HB, self.configSep, self.dataFolder = OR_per_HB, configSep, dataFolder
+
+
+def GenerateHeatBathGaugeConfigurations(params, HBparams, seed: int = 1) -> int:
+    lib = C.load()
+    return lib.lgf_dropin_generate_heatbath(_shape(params.shape), params.beta, HBparams.start, HBparams.stop,
+                                            HBparams.ThermSteps, HBparams.OR_per_HB, HBparams.configSep,
+                                            HBparams.dataFolder.encode(), ctypes.c_uint64(seed))
 
 
 def MeasureFlowedGaugeConfigurations(params, flowParams) -> int:
