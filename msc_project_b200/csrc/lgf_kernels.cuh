@@ -32,8 +32,11 @@
 #ifndef LGF_STAGE_MINB
 #define LGF_STAGE_MINB 1
 #endif
-#ifndef LGF_MEAS_MINB
-#define LGF_MEAS_MINB 2  // 2 blocks of 192 per SM: measured faster than 1 block without a register cap
+#ifndef LGF_MEAS_MINB_D
+#define LGF_MEAS_MINB_D 2  // double: resident measurement blocks per SM (caps registers)
+#endif
+#ifndef LGF_MEAS_MINB_F
+#define LGF_MEAS_MINB_F 2  // float
 #endif
 
 namespace lgf {
@@ -433,8 +436,11 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
 //   q(x) = ReTr(F^32 F^01) + ReTr(F^31 F^20) + ReTr(F^30 F^12)
 //        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
 //                                             (TopologicalCharge.cpp:11-16)
+template <typename R> struct MeasMinBlocks { static constexpr int value = LGF_MEAS_MINB_F; };
+template <> struct MeasMinBlocks<double> { static constexpr int value = LGF_MEAS_MINB_D; };
+
 template <typename R, bool OUT = false>
-__global__ void __launch_bounds__(MEAS_SITES * 6, LGF_MEAS_MINB) k_measure(const LatDesc<R>* __restrict__ descs,
+__global__ void __launch_bounds__(MEAS_SITES * 6, MeasMinBlocks<R>::value) k_measure(const LatDesc<R>* __restrict__ descs,
                                                                            const int4* __restrict__ mtiles,
                                                                            const int* __restrict__ nmtiles,
                                                                            MeasOut out) {
