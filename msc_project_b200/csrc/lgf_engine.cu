@@ -54,8 +54,7 @@ size_t footprint_bytes(const int shape[4], int precision, int meas_slots) {
 int default_threads(int precision) { return precision == LGF_PREC_FP64 ? 128 : 128; }
 
 void buf_free(LatticeBuf& b) {
-    for (int i = 0; i < 3; ++i)
-        if (b.U[i]) cudaFree(b.U[i]);
+    if (b.U[0]) cudaFree(b.U[0]);  // U[1], U[2] lie in the same allocation
     if (b.A) cudaFree(b.A);
     if (b.partial) cudaFree(b.partial);
     if (b.slice_sums) cudaFree(b.slice_sums);
@@ -72,7 +71,14 @@ int buf_alloc(lgf_ctx* ctx, LatticeBuf& b, const int shape[4], int precision, in
     const size_t rs = real_size(precision);
     b.nchunk = (b.g.Vs + MEAS_SITES - 1) / MEAS_SITES;
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMalloc(&b.U[i], V * 4 * 18 * rs);
+    // the link ring as one allocation: U1 (FP64) or U1..U2 (FP32) then spans
+    // exactly V*4*18 doubles, the upload/download staging area
+    const size_t ring = V * 4 * 18 * rs;
+    e = cudaMalloc(&b.U[0], 3 * ring);
+    if (e == cudaSuccess) {
+        b.U[1] = (char*)b.U[0] + ring;
+        b.U[2] = (char*)b.U[0] + 2 * ring;
+    }
     if (e == cudaSuccess) e = cudaMalloc(&b.A, V * 4 * 8 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&b.partial, (size_t)b.g.n[0] * b.nchunk * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&b.slice_sums, (size_t)b.g.n[0] * sizeof(double2));
@@ -426,8 +432,15 @@ int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b) {
 
 // Links cross the PCIe/C2C link as float64 file order; the reorder to the
 // SoA layout (and the float conversion of the mixed form) runs on the GPU.
-// Chunked through a pinned staging buffer so host memory is not pinned.
-static const size_t STAGE_BYTES = 64u << 20;
+// The file-order copy is staged in the lattice's own ring: between flows the
+// links live in U0 and U1 (FP64) or U1..U2 (FP32) is scratch of exactly the
+// file size, so an upload or download allocates no device memory.  A
+// page-locked caller buffer is one DMA; pageable memory goes through the
+// context's two pinned chunks, the host copy of one chunk overlapping the
+// DMA of the other.
+static const size_t PIN_CHUNK = 32u << 20;
+
+static double* file_staging(const LatticeBuf& b) { return (double*)b.U[1]; }
 
 static bool is_pinned(const void* p) {
     cudaPointerAttributes a;
@@ -438,71 +451,92 @@ static bool is_pinned(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+static cudaError_t ensure_pinned_chunks(lgf_ctx* ctx) {
+    if (ctx->pin[0]) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaMallocHost(&ctx->pin[k], PIN_CHUNK);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->pin_done[k], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) release_pinned_chunks(ctx);
+    return e;
+}
+
+void release_pinned_chunks(lgf_ctx* ctx) {
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->pin_done[k]) cudaEventDestroy(ctx->pin_done[k]);
+        if (ctx->pin[k]) cudaFreeHost(ctx->pin[k]);
+        ctx->pin_done[k] = nullptr;
+        ctx->pin[k] = nullptr;
+    }
+}
+
 int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host) {
     const size_t bytes = (size_t)b.g.V * 4 * 18 * sizeof(double);
-    double* dev = nullptr;
-    LGF_CUDA_TRY(ctx, cudaMallocAsync((void**)&dev, bytes, ctx->stream));
-    if (is_pinned(host)) {  // page-locked caller buffer: one direct DMA
-        cudaError_t e = cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
-        int rc = e == cudaSuccess ? launch_to_device(ctx, b, dev)
-                                  : set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
-        cudaFreeAsync(dev, ctx->stream);
-        e = cudaStreamSynchronize(ctx->stream);
-        if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
-        return rc;
+    char* stage = (char*)file_staging(b);
+    cudaError_t e = cudaSuccess;
+    if (is_pinned(host)) {
+        e = cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    } else {
+        std::lock_guard<std::mutex> lk(ctx->pin_mu);
+        e = ensure_pinned_chunks(ctx);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, LGF_ENOMEM, "pinned staging allocation failed: %s", cudaGetErrorString(e));
+        }
+        for (size_t off = 0, i = 0; off < bytes && e == cudaSuccess; off += PIN_CHUNK, ++i) {
+            const size_t n = std::min(PIN_CHUNK, bytes - off);
+            const int k = (int)(i & 1);
+            e = cudaEventSynchronize(ctx->pin_done[k]);  // the DMA that last read chunk k has finished
+            if (e != cudaSuccess) break;
+            std::memcpy(ctx->pin[k], (const char*)host + off, n);
+            e = cudaMemcpyAsync(stage + off, ctx->pin[k], n, cudaMemcpyHostToDevice, ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->pin_done[k], ctx->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // chunks free for the next caller
     }
-    void* pin = nullptr;
-    const size_t chunk = std::min(bytes, STAGE_BYTES);
-    cudaError_t e = cudaMallocHost(&pin, chunk);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(dev, ctx->stream);
-        return set_error(ctx, LGF_ENOMEM, "pinned staging allocation failed: %s", cudaGetErrorString(e));
-    }
-    for (size_t off = 0; off < bytes && e == cudaSuccess; off += chunk) {
-        const size_t n = std::min(chunk, bytes - off);
-        e = cudaStreamSynchronize(ctx->stream);  // staging buffer free again
-        if (e != cudaSuccess) break;
-        std::memcpy(pin, (const char*)host + off, n);
-        e = cudaMemcpyAsync((char*)dev + off, pin, n, cudaMemcpyHostToDevice, ctx->stream);
-    }
-    int rc = LGF_OK;
-    if (e == cudaSuccess) rc = launch_to_device(ctx, b, dev);
-    else rc = set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
-    cudaFreeAsync(dev, ctx->stream);
-    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
-    cudaFreeHost(pin);
-    if (rc == LGF_OK && e2 != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e2));
+    if (e != cudaSuccess) return set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
+    int rc = launch_to_device(ctx, b, (const double*)stage);
+    e = cudaStreamSynchronize(ctx->stream);
+    if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
     return rc;
 }
 
 int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host) {
     const size_t bytes = (size_t)b.g.V * 4 * 18 * sizeof(double);
-    double* dev = nullptr;
-    LGF_CUDA_TRY(ctx, cudaMallocAsync((void**)&dev, bytes, ctx->stream));
-    int rc = launch_to_file(ctx, b, dev);
-    if (rc == LGF_OK && is_pinned(host)) {
-        cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-        cudaFreeAsync(dev, ctx->stream);
-        cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess || e2 != cudaSuccess)
-            rc = set_error(ctx, LGF_ECUDA, "download failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
-        return rc;
-    }
-    void* pin = nullptr;
-    const size_t chunk = std::min(bytes, STAGE_BYTES);
-    cudaError_t e = cudaMallocHost(&pin, chunk);
-    for (size_t off = 0; rc == LGF_OK && e == cudaSuccess && off < bytes; off += chunk) {
-        const size_t n = std::min(chunk, bytes - off);
-        e = cudaMemcpyAsync(pin, (const char*)dev + off, n, cudaMemcpyDeviceToHost, ctx->stream);
+    char* stage = (char*)file_staging(b);
+    int rc = launch_to_file(ctx, b, (double*)stage);
+    if (rc != LGF_OK) return rc;
+    cudaError_t e = cudaSuccess;
+    if (is_pinned(host)) {
+        e = cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-        if (e == cudaSuccess) std::memcpy((char*)host + off, pin, n);
+    } else {
+        std::lock_guard<std::mutex> lk(ctx->pin_mu);
+        e = ensure_pinned_chunks(ctx);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, LGF_ENOMEM, "pinned staging allocation failed: %s", cudaGetErrorString(e));
+        }
+        // chunk i+1 is copied to the device-side buffer while the host drains chunk i
+        const size_t nchunks = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
+        auto issue = [&](size_t i) {
+            const size_t off = i * PIN_CHUNK, n = std::min(PIN_CHUNK, bytes - off);
+            cudaError_t r = cudaMemcpyAsync(ctx->pin[i & 1], stage + off, n, cudaMemcpyDeviceToHost, ctx->stream);
+            return r == cudaSuccess ? cudaEventRecord(ctx->pin_done[i & 1], ctx->stream) : r;
+        };
+        e = issue(0);
+        for (size_t i = 0; i < nchunks && e == cudaSuccess; ++i) {
+            if (i + 1 < nchunks) e = issue(i + 1);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ctx->pin_done[i & 1]);
+            if (e != cudaSuccess) break;
+            const size_t off = i * PIN_CHUNK;
+            std::memcpy((char*)host + off, ctx->pin[i & 1], std::min(PIN_CHUNK, bytes - off));
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
-    cudaFreeAsync(dev, ctx->stream);
-    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
-    if (pin) cudaFreeHost(pin);
-    if (rc == LGF_OK && (e != cudaSuccess || e2 != cudaSuccess))
-        rc = set_error(ctx, LGF_ECUDA, "download failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
-    return rc;
+    if (e != cudaSuccess) return set_error(ctx, LGF_ECUDA, "download failed: %s", cudaGetErrorString(e));
+    return LGF_OK;
 }
 
 }  // namespace lgf
@@ -582,6 +616,7 @@ int lgf_ctx_destroy(lgf_ctx* ctx) {
     if (!ctx) return LGF_EINVAL;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    release_pinned_chunks(ctx);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return LGF_OK;

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,11 @@ struct lgf_ctx {
     int sm_count = 0;
     std::string err;
     int tuned_threads[2] = {0, 0};  // per precision; 0 = not tuned yet
+    // two pinned host chunks for uploads/downloads from pageable memory
+    // (allocated on first use; a server's worker shares them, hence the lock)
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_done[2] = {nullptr, nullptr};
+    std::mutex pin_mu;
 };
 
 namespace lgf {
@@ -81,9 +87,10 @@ int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file_order);
 int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file_order);
 int launch_generate(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale);
 
-// host->device upload of file-order links through a pinned staging buffer
+// host<->device copies of file-order links, staged in the lattice's ring
 int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host);
 int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host);
+void release_pinned_chunks(lgf_ctx* ctx);
 
 // measurement schedule of FlowSavedGaugeConfigurations for one job
 int count_measurements(const lgf_flow_opts& o);

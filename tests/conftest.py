@@ -40,3 +40,22 @@ def q_err(a, b):
 def rel_err(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return float(np.max(np.abs(a - b) / np.abs(b)))
+
+
+def random_gauge(U, shape, seed):
+    """U'_mu(x) = g(x) U_mu(x) g(x+mu)^dag with random SU(3) g (host numpy)."""
+    from oracle import oracle as O
+    V = O.volume(shape)
+    g = O.generate_G(shape, seed, 1.0).reshape(V, 4, 18)[:, 0]
+    G = g[:, 0::2] + 1j * g[:, 1::2]
+    G = G.reshape(V, 3, 3)
+    M = (U.reshape(V, 4, 18)[:, :, 0::2] + 1j * U.reshape(V, 4, 18)[:, :, 1::2]).reshape(V, 4, 3, 3)
+    idx = np.arange(V).reshape(shape)
+    out = np.empty_like(M)
+    for mu in range(4):
+        nb = np.roll(idx, -1, axis=mu).reshape(-1)
+        out[:, mu] = G @ M[:, mu] @ np.conj(np.transpose(G[nb], (0, 2, 1)))
+    r = np.empty((V, 4, 9, 2))
+    r[..., 0] = out.reshape(V, 4, 9).real
+    r[..., 1] = out.reshape(V, 4, 9).imag
+    return r.reshape(-1)

@@ -13,7 +13,7 @@ from pathlib import Path
 
 import numpy as np
 import pytest
-from conftest import GOLDEN, golden_json, golden_links, q_err, rel_err
+from conftest import GOLDEN, golden_json, golden_links, q_err, random_gauge, rel_err
 
 from msc_project_b200 import FP32MIXED, FP64, Job
 from oracle import oracle as O
@@ -249,24 +249,6 @@ def test_dropin_measure_flowed_outputs_read_like_the_analysis(ctx, tmp_path):
 
 
 # ------------------------------------------------------------- properties
-def random_gauge(U, shape, seed):
-    """U'_mu(x) = g(x) U_mu(x) g(x+mu)^dag with random SU(3) g (host numpy)."""
-    V = O.volume(shape)
-    g = O.generate_G(shape, seed, 1.0).reshape(V, 4, 18)[:, 0]
-    G = g[:, 0::2] + 1j * g[:, 1::2]
-    G = G.reshape(V, 3, 3)
-    M = (U.reshape(V, 4, 18)[:, :, 0::2] + 1j * U.reshape(V, 4, 18)[:, :, 1::2]).reshape(V, 4, 3, 3)
-    idx = np.arange(V).reshape(shape)
-    out = np.empty_like(M)
-    for mu in range(4):
-        nb = np.roll(idx, -1, axis=mu).reshape(-1)
-        out[:, mu] = G @ M[:, mu] @ np.conj(np.transpose(G[nb], (0, 2, 1)))
-    r = np.empty((V, 4, 9, 2))
-    r[..., 0] = out.reshape(V, 4, 9).real
-    r[..., 1] = out.reshape(V, 4, 9).imag
-    return r.reshape(-1)
-
-
 def test_gauge_invariance_and_parity(ctx):
     shape = (8, 8, 8, 8)
     U = golden_links("hb8_seed1.bin")
