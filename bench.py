@@ -11,7 +11,10 @@ included).  `value`: device time of the flow launches with the links resident
 in HBM (CUDA events on the engine's stream), summed over the K timed jobs,
 max over ranks.  `e2e`: the same jobs through the public C ABI from pinned
 host memory -- upload of the configuration, the flow, and the read-back of
-E(t), Q(t) -- timed on the host around the synchronous calls.
+E(t), Q(t) -- timed on the host around the synchronous calls.  `flow_only`:
+the same 300 steps without measurements.  Forms (rank 0 at N=1): FP32-mixed
+on 32^4, the batched 64-configuration ensemble, a served Poisson stream at a
+sweep of arrival rates, and heatbath generation.
 
 --impl reference runs the LGF reference itself (oracle/_ref/lgf_ref, the
 unmodified sources) on the host cores: one single-rank process per core,
@@ -380,6 +383,15 @@ def engine_arm(args):
     dev_s = reduce_max(dist, dev_s)
     value = world * V * NSTEPS * args.steps / dev_s
 
+    # ---- the flow alone (no measurements), device-timed like the job
+    lat.flow(EPS, 30, 0, 0.0, False, reunit)
+    secs_fo = 0.0
+    for _ in range(2):
+        lat.flow(EPS, NSTEPS, 0, 0.0, False, reunit)
+        ctx.check(ctx.lib.lgf_last_flow_seconds(lat.h, ctypes.byref(secs)))
+        secs_fo += secs.value
+    flow_only = world * V * NSTEPS * 2 / reduce_max(dist, secs_fo)
+
     # ---- end to end through the public ABI from pinned host memory
     import torch
     host = torch.empty(V * 72, dtype=torch.float64, pin_memory=True)
@@ -424,8 +436,9 @@ def engine_arm(args):
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
+        rates = [float(r) for r in args.serve_rates.split(",") if r]
         forms = {"fp32mixed": form_fp32mixed(ctx), "batched": form_batched(ctx),
-                 "served": form_served(ctx, args.serve_jobs, args.serve_rate), "heatbath": form_heatbath(ctx)}
+                 "served": [form_served(ctx, args.serve_jobs, r) for r in rates], "heatbath": form_heatbath(ctx)}
 
     launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
     line = {
@@ -438,7 +451,12 @@ def engine_arm(args):
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "site-RK3-steps/s", "h2d_bytes_per_step": V * 72 * 8,
                 "d2h_bytes_per_step": nmeas * 3 * 8},
-        "roofline": {"bound": "hbm", "kernel": "k_rk3_stage (mean of the 3 stages)", "achieved": achieved,
+        "flow_only": {"value": flow_only, "unit": "site-RK3-steps/s",
+                      "note": "the same 300 steps without E/Q measurements (device time)"},
+        "roofline": {"bound": "hbm", "binding": f"fp64 FMA pipe (fp64_pipe below): one stage is "
+                     f"{V * FLOPS_PER_SITE_STAGE / (fma_peak * 1e12) * 1e3:.3f} ms of FP64 FMA work at peak and "
+                     f"{stage_bytes / (hbm_peak * 1e9) * 1e3:.3f} ms of HBM traffic at the measured copy rate",
+                     "kernel": "k_rk3_stage (mean of the 3 stages)", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
                      "traffic": NCU_STAGE_TRAFFIC_BYTES[prec], "traffic_note": "DRAM bytes of one stage-2 launch (ncu), algorithmic 1104 MB (FP64) / 552 MB (FP32)", "stage_ms": stage_ms, "measure_ms": ms[3]},
         "fp64_pipe": {"achieved_tflops": stage_tflops, "nominal_peak_tflops_at_clock": fma_peak,
@@ -482,8 +500,8 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, batched and served forms")
-    ap.add_argument("--serve-jobs", type=int, default=12)
-    ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson arrival rate, jobs/s")
+    ap.add_argument("--serve-jobs", type=int, default=10, help="jobs per arrival rate of the served form")
+    ap.add_argument("--serve-rates", default="0.25,1.0", help="Poisson arrival rates (jobs/s) swept by the served form")
     ap.add_argument("--profile", action="store_true", help="one launch of each kernel (for ncu captures)")
     ap.add_argument("--profile-reps", type=int, default=1)
     args = ap.parse_args()
