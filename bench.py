@@ -12,8 +12,8 @@ in HBM (CUDA events on the engine's stream), summed over the K timed jobs,
 max over ranks.  `e2e`: the same jobs through the public C ABI from pinned
 host memory -- upload of the configuration, the flow, and the read-back of
 E(t), Q(t) -- timed on the host around the synchronous calls.  `flow_only`:
-the same 300 steps without measurements.  Forms (rank 0 at N=1): FP32-mixed
-on 32^4, the batched 64-configuration ensemble, a served Poisson stream at a
+the same 300 steps without measurements.  Forms (rank 0 at N=1): FP64 rate
+against volume (16^4 to 48^4), FP32-mixed on 32^4, the batched 64-configuration ensemble, a served Poisson stream at a
 sweep of arrival rates, and heatbath generation.
 
 --impl reference runs the LGF reference itself (oracle/_ref/lgf_ref, the
@@ -237,6 +237,27 @@ def form_fp32mixed(ctx):
                       "dE/E<1e-5": bool(np.max(np.abs(r32.E - r64.E) / np.abs(r64.E)) < 1e-5)}}
 
 
+def form_volumes(ctx):
+    """FP64 throughput against volume: 16^4, 24^3x48, 32^4 and 48^4 (generator
+    G seed 7), eps 0.01, 100 RK3 steps, E/Q at t=0 and every 10 steps, and the
+    same 100 steps without measurements."""
+    import numpy as np
+    from msc_project_b200 import FP64
+    out = []
+    secs = ctypes.c_double()
+    for shape in ((16, 16, 16, 16), (48, 24, 24, 24), (32, 32, 32, 32), (48, 48, 48, 48)):
+        V = int(np.prod(shape))
+        with ctx.lattice(shape, FP64) as lat:
+            lat.generate(7, 0.5)
+            _flow_timed(ctx, lat, 0.01, 10, 10)  # warm-up: graph capture for this lattice
+            _, sec = _flow_timed(ctx, lat, 0.01, 100, 10)
+            lat.flow(0.01, 100, 0, 0.0, False, 0)
+            ctx.check(ctx.lib.lgf_last_flow_seconds(lat.h, ctypes.byref(secs)))
+        out.append({"shape": list(shape), "sites": V, "site_steps_per_s": V * 100 / sec,
+                    "flow_only_site_steps_per_s": V * 100 / secs.value})
+    return out
+
+
 ENSEMBLE = [((8, 8, 8, 8), 16), ((12, 12, 12, 12), 16), ((16, 16, 16, 16), 16), ((32, 16, 16, 16), 8),
             ((48, 24, 24, 24), 8)]
 
@@ -437,8 +458,12 @@ def engine_arm(args):
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         rates = [float(r) for r in args.serve_rates.split(",") if r]
-        forms = {"fp32mixed": form_fp32mixed(ctx), "batched": form_batched(ctx),
-                 "served": [form_served(ctx, args.serve_jobs, r) for r in rates], "heatbath": form_heatbath(ctx)}
+        makers = {"volumes_fp64": lambda: form_volumes(ctx), "fp32mixed": lambda: form_fp32mixed(ctx),
+                  "batched": lambda: form_batched(ctx),
+                  "served": lambda: [form_served(ctx, args.serve_jobs, r) for r in rates],
+                  "heatbath": lambda: form_heatbath(ctx)}
+        wanted = list(makers) if args.forms == "all" else args.forms.split(",")
+        forms = {k: makers[k]() for k in wanted}
 
     launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
     line = {
@@ -499,7 +524,8 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "fp32mixed"], default="fp64")
     ap.add_argument("--ref-procs", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, batched and served forms")
+    ap.add_argument("--no-forms", action="store_true", help="skip the forms (volumes, FP32-mixed, batched, served, heatbath)")
+    ap.add_argument("--forms", default="all", help="comma list of forms to run (default all)")
     ap.add_argument("--serve-jobs", type=int, default=10, help="jobs per arrival rate of the served form")
     ap.add_argument("--serve-rates", default="0.25,1.0", help="Poisson arrival rates (jobs/s) swept by the served form")
     ap.add_argument("--profile", action="store_true", help="one launch of each kernel (for ncu captures)")
