@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -41,11 +42,11 @@ bool valid_shape(const int shape[4]) {
 static size_t real_size(int prec) { return prec == LGF_PREC_FP64 ? sizeof(double) : sizeof(float); }
 
 size_t footprint_bytes(const int shape[4], int precision, int meas_slots) {
-    const size_t V = (size_t)shape[0] * shape[1] * shape[2] * shape[3];
+    const size_t V = (size_t)shape[0] * shape[1] * shape[2] * shape[3], Vp = padded_sites(V);
     const size_t rs = real_size(precision);
     const size_t nchunk = ((size_t)shape[1] * shape[2] * shape[3] + MEAS_SITES - 1) / MEAS_SITES;
-    size_t b = 3 * V * 4 * 18 * rs;              // link ring
-    b += V * 4 * 8 * rs;                          // su(3) accumulator
+    size_t b = 3 * Vp * 4 * 18 * rs;             // link ring
+    b += Vp * 4 * 8 * rs;                         // su(3) accumulator
     b += (size_t)shape[0] * nchunk * sizeof(double2) + (size_t)shape[0] * sizeof(double2);
     b += (size_t)std::max(meas_slots, 1) * (2 + 2 * (size_t)shape[0]) * sizeof(double) + 256;
     return b;
@@ -67,19 +68,19 @@ int buf_alloc(lgf_ctx* ctx, LatticeBuf& b, const int shape[4], int precision, in
     b = LatticeBuf();
     b.g = make_geom(shape);
     b.prec = precision;
-    const size_t V = (size_t)b.g.V;
+    const size_t Vp = padded_sites((size_t)b.g.V);  // the layout's whole 32-site blocks
     const size_t rs = real_size(precision);
     b.nchunk = (b.g.Vs + MEAS_SITES - 1) / MEAS_SITES;
     cudaError_t e = cudaSuccess;
     // the link ring as one allocation: U1 (FP64) or U1..U2 (FP32) then spans
-    // exactly V*4*18 doubles, the upload/download staging area
-    const size_t ring = V * 4 * 18 * rs;
+    // at least V*4*18 doubles, the upload/download staging area
+    const size_t ring = Vp * 4 * 18 * rs;
     e = cudaMalloc(&b.U[0], 3 * ring);
     if (e == cudaSuccess) {
         b.U[1] = (char*)b.U[0] + ring;
         b.U[2] = (char*)b.U[0] + 2 * ring;
     }
-    if (e == cudaSuccess) e = cudaMalloc(&b.A, V * 4 * 8 * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&b.A, Vp * 4 * 8 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&b.partial, (size_t)b.g.n[0] * b.nchunk * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&b.slice_sums, (size_t)b.g.n[0] * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&b.slot, sizeof(int));
@@ -122,7 +123,7 @@ int count_measurements(const lgf_flow_opts& o) {
 // L2 reuse distance of the stencil.  In plain site order the x0 +- 1 (and, in
 // the measurement, up to +- 3) neighbours of a site are reused one slice of
 // work later; once a slice of work exceeds the L2 budget they come from HBM
-// again.  Large lattices are therefore ordered in blocks of whole x1 rows,
+// again.  Large lattices are therefore ordered in blocks of x1 (and x2) rows,
 // each block swept through every x0 slice before the next block starts.  Only
 // the order changes: the set of tiles is the same, and no result depends on
 // it (no reduction runs in tile order).
@@ -138,31 +139,56 @@ int count_measurements(const lgf_flow_opts& o) {
 static const double STAGE_L2_BUDGET = LGF_STAGE_L2_MB * double(1 << 20);
 static const double MEAS_L2_BUDGET = LGF_MEAS_L2_MB * double(1 << 20);
 
-static long long block_sites(const Geom& g, double budget, double bytes_per_site) {
-    const long long Vs = g.Vs;
-    if ((double)Vs * bytes_per_site <= budget) return Vs;  // one block = the natural order
-    const long long row = (long long)g.n[2] * g.n[3];
-    const long long B = std::max((long long)(budget / bytes_per_site) / row, 1LL) * row;
-    return std::min(B, Vs);
+// A block: x1 in [a1, b1), x2 in [a2, b2), all x3.  One block per slice when
+// a slice of work fits the budget; else blocks of whole x1 rows, at least
+// MIN_ROWS deep so that most x1 neighbours stay inside; else (lattices whose
+// x1 rows are themselves large) square (x1, x2) blocks.
+struct SiteBlock { int a1, b1, a2, b2; };
+#ifndef LGF_MIN_ROWS
+#define LGF_MIN_ROWS 4
+#endif
+static const int MIN_ROWS = LGF_MIN_ROWS;
+
+static std::vector<SiteBlock> site_blocks(const Geom& g, double budget, double bytes_per_site) {
+    std::vector<SiteBlock> out;
+    const int N1 = g.n[1], N2 = g.n[2], N3 = g.n[3];
+    const double sites = budget / bytes_per_site;  // sites of one block and slice
+    if ((double)g.Vs <= sites) {
+        out.push_back({0, N1, 0, N2});
+    } else if ((double)MIN_ROWS * N2 * N3 <= sites) {
+        const int r = std::max(1, (int)(sites / ((double)N2 * N3)));
+        for (int a = 0; a < N1; a += r) out.push_back({a, std::min(a + r, N1), 0, N2});
+    } else {
+        const int side = std::max(1, (int)std::sqrt(sites / N3));
+        for (int a = 0; a < N1; a += side)
+            for (int c = 0; c < N2; c += side) out.push_back({a, std::min(a + side, N1), c, std::min(c + side, N2)});
+    }
+    return out;
 }
 
-// stage tiles of T consecutive sites (first site a multiple of T) of lattice i
+// stage tiles of T consecutive sites (first site a multiple of T) of lattice
+// i, each assigned to the block row that holds its first site
 static void append_stage_tiles(std::vector<int2>& tiles, int i, const Geom& g, int T, double bytes_per_site) {
-    const long long Vs = g.Vs, B = block_sites(g, STAGE_L2_BUDGET, bytes_per_site);
-    for (long long k0 = 0; k0 < Vs; k0 += B)
-        for (long long x0 = 0; x0 < g.n[0]; ++x0) {
-            const long long lo = x0 * Vs + k0, hi = x0 * Vs + std::min(k0 + B, Vs);
-            for (long long s0 = (lo + T - 1) / T * T; s0 < hi; s0 += T) tiles.push_back(make_int2(i, (int)s0));
-        }
+    const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
+    for (const SiteBlock& b : site_blocks(g, STAGE_L2_BUDGET, bytes_per_site))
+        for (long long x0 = 0; x0 < g.n[0]; ++x0)
+            for (long long x1 = b.a1; x1 < b.b1; ++x1) {
+                const long long base = x0 * g.Vs + x1 * row;
+                const long long lo = base + b.a2 * N3, hi = base + b.b2 * N3;
+                for (long long s0 = (lo + T - 1) / T * T; s0 < hi; s0 += T) tiles.push_back(make_int2(i, (int)s0));
+            }
 }
 
 // measurement tiles (lattice, slice, 32-site chunk of the slice) of lattice i
-static void append_measure_tiles(std::vector<int4>& tiles, int i, const Geom& g, int nchunk, double bytes_per_site) {
-    const long long cb = std::max(block_sites(g, MEAS_L2_BUDGET, bytes_per_site) / MEAS_SITES, 1LL);
-    for (long long c0 = 0; c0 < nchunk; c0 += cb)
+static void append_measure_tiles(std::vector<int4>& tiles, int i, const Geom& g, double bytes_per_site) {
+    const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
+    for (const SiteBlock& b : site_blocks(g, MEAS_L2_BUDGET, bytes_per_site))
         for (int t = 0; t < g.n[0]; ++t)
-            for (long long c = c0; c < std::min(c0 + cb, (long long)nchunk); ++c)
-                tiles.push_back(make_int4(i, t, (int)c, 0));
+            for (long long x1 = b.a1; x1 < b.b1; ++x1) {
+                const long long lo = x1 * row + b.a2 * N3, hi = x1 * row + b.b2 * N3;
+                for (long long c = (lo + MEAS_SITES - 1) / MEAS_SITES; c * MEAS_SITES < hi; ++c)
+                    tiles.push_back(make_int4(i, t, (int)c, 0));
+            }
 }
 
 // ------------------------------------------------------------------ groups
@@ -280,7 +306,7 @@ public:
         h_jobs_.clear();
         for (int i : which) {
             const LatticeBuf& b = *members_[i];
-            append_measure_tiles(h_mtiles_, i, b.g, b.nchunk, 4.0 * 18 * sizeof(R));
+            append_measure_tiles(h_mtiles_, i, b.g, 4.0 * 18 * sizeof(R));
             for (int t = 0; t < b.g.n[0]; ++t) h_rtiles_.push_back(make_int2(i, t));
             h_jobs_.push_back(i);
         }
@@ -478,9 +504,9 @@ int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b) {
 }
 
 // Links cross the PCIe/C2C link as float64 file order; the reorder to the
-// SoA layout (and the float conversion of the mixed form) runs on the GPU.
+// device layout (and the float conversion of the mixed form) runs on the GPU.
 // The file-order copy is staged in the lattice's own ring: between flows the
-// links live in U0 and U1 (FP64) or U1..U2 (FP32) is scratch of exactly the
+// links live in U0 and U1 (FP64) or U1..U2 (FP32) is scratch of at least the
 // file size, so an upload or download allocates no device memory.  A
 // page-locked caller buffer is one DMA; pageable memory goes through the
 // context's two pinned chunks, the host copy of one chunk overlapping the

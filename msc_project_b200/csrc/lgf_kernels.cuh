@@ -16,7 +16,7 @@
 //   k_reduce_slices / k_reduce_total
 //                      fixed-order FP64 reductions (per x0 slice, then global)
 //                      in place of MPI_Allreduce; deterministic run to run.
-//   k_to_device / k_to_file    file-order float64 <-> device SoA layout
+//   k_to_device / k_to_file    file-order float64 <-> device layout
 //   k_generate_G       synthetic links exp(i s sum_a h_a T^a)
 //   k_reunitarize      FP32-mixed: Gram-Schmidt rows 0,1; row 2 = conj(r0 x r1)
 //   k_unitarity        max ||U^dag U - 1||_F and |det U - 1| per block
@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_total(const LatDesc<R>* 
 }
 
 // ------------------------------------------------------------- layouts
-// file order (double, [s][mu][k][re,im]) -> device SoA in precision R
+// file order (double, [s][mu][k][re,im]) -> device layout in precision R
 template <typename R>
 __global__ void k_to_device(const double2* __restrict__ file, cplx<R>* __restrict__ U, int V) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -620,7 +620,7 @@ __global__ void k_to_device(const double2* __restrict__ file, cplx<R>* __restric
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
         const double2 v = src[k];
-        U[((size_t)mu * 9 + k) * V + s] = cmk<R>((R)v.x, (R)v.y);
+        U[link_offset(mu, k, s)] = cmk<R>((R)v.x, (R)v.y);
     }
 }
 template <typename R>
@@ -631,7 +631,7 @@ __global__ void k_to_file(const cplx<R>* __restrict__ U, double2* __restrict__ f
     double2* dst = file + ((size_t)s * 4 + mu) * 9;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        const cplx<R> z = U[((size_t)mu * 9 + k) * V + s];
+        const cplx<R> z = U[link_offset(mu, k, s)];
         dst[k] = make_double2((double)z.re, (double)z.im);
     }
 }

@@ -6,11 +6,15 @@
 // periodic wrap in every direction (the "torus" type, Lattice.cpp:447-459).
 // One GPU holds the whole lattice, so there is no halo exchange.
 //
-// Device layout (structure of arrays, one complex entry per load):
-//   links  cplx<R>  U[(mu*9 + k) * V + s]        k = 3*row + col
-//   su(3)  R        A[(mu*8 + c) * V + s]        8 coordinates (lgf_su3.cuh)
-// so a warp of 32 consecutive sites reads 32 consecutive complex entries
-// (512 B for double, 256 B for float) per load instruction.
+// Device layout: blocks of 32 consecutive sites, each block holding every
+// entry of its sites' four links (structure of arrays inside the block):
+//   links  cplx<R>  U[((s/32)*36 + mu*9 + k) * 32 + s%32]    k = 3*row + col
+//   su(3)  R        A[((s/32)*32 + mu*8 + c) * 32 + s%32]    8 coordinates (lgf_su3.cuh)
+// A warp of 32 consecutive sites still reads 32 consecutive complex entries
+// (512 B for double, 256 B for float) per load instruction, and the links of
+// a site range sit together (18 KB per block in double) instead of in 36
+// arrays of V entries each: a stencil over a large lattice touches a few
+// pages per neighbour instead of dozens.  Buffers hold padded_sites(V) sites.
 #pragma once
 #include <stdint.h>
 #include "lgf_su3.cuh"
@@ -93,29 +97,40 @@ template <typename R> __device__ __forceinline__ void stc(cplx<R>* p, cplx<R> z)
     *reinterpret_cast<V2*>(p) = v;
 }
 
+constexpr int LAYOUT_BLOCK = 32;  // sites per layout block
+__host__ __device__ __forceinline__ size_t padded_sites(size_t V) { return (V + LAYOUT_BLOCK - 1) / LAYOUT_BLOCK * LAYOUT_BLOCK; }
+// offset of complex entry k of link mu at site s; entry k+1 is LAYOUT_BLOCK further
+__host__ __device__ __forceinline__ size_t link_offset(int mu, int k, int s) {
+    return ((size_t)(s / LAYOUT_BLOCK) * 36 + mu * 9 + k) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
+}
+__host__ __device__ __forceinline__ size_t alg_offset(int mu, int c, int s) {
+    return ((size_t)(s / LAYOUT_BLOCK) * 32 + mu * 8 + c) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
+}
+
+// (V is kept in the signatures: the lattice volume, no longer a stride)
 template <typename R> __device__ __forceinline__ su3<R> load_link(const cplx<R>* __restrict__ U, int V, int mu, int s) {
     su3<R> a;
-    const cplx<R>* p = U + (size_t)mu * 9 * V + s;
+    const cplx<R>* p = U + link_offset(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) a.m[k] = ldc(p + (size_t)k * V);
+    for (int k = 0; k < 9; ++k) a.m[k] = ldc(p + k * LAYOUT_BLOCK);
     return a;
 }
 template <typename R> __device__ __forceinline__ void store_link(cplx<R>* __restrict__ U, int V, int mu, int s, const su3<R>& a) {
-    cplx<R>* p = U + (size_t)mu * 9 * V + s;
+    cplx<R>* p = U + link_offset(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) stc(p + (size_t)k * V, a.m[k]);
+    for (int k = 0; k < 9; ++k) stc(p + k * LAYOUT_BLOCK, a.m[k]);
 }
 template <typename R> __device__ __forceinline__ alg<R> load_alg(const R* __restrict__ A, int V, int mu, int s) {
     alg<R> z;
-    const R* p = A + (size_t)mu * 8 * V + s;
+    const R* p = A + alg_offset(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) z.v[k] = __ldg(p + (size_t)k * V);
+    for (int k = 0; k < 8; ++k) z.v[k] = __ldg(p + k * LAYOUT_BLOCK);
     return z;
 }
 template <typename R> __device__ __forceinline__ void store_alg(R* __restrict__ A, int V, int mu, int s, const alg<R>& z) {
-    R* p = A + (size_t)mu * 8 * V + s;
+    R* p = A + alg_offset(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) p[(size_t)k * V] = z.v[k];
+    for (int k = 0; k < 8; ++k) p[k * LAYOUT_BLOCK] = z.v[k];
 }
 
 }  // namespace lgf
