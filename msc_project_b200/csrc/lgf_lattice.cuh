@@ -97,7 +97,10 @@ template <typename R> __device__ __forceinline__ void stc(cplx<R>* p, cplx<R> z)
     *reinterpret_cast<V2*>(p) = v;
 }
 
-constexpr int LAYOUT_BLOCK = 32;  // sites per layout block
+#ifndef LGF_LAYOUT_BLOCK
+#define LGF_LAYOUT_BLOCK 32
+#endif
+constexpr int LAYOUT_BLOCK = LGF_LAYOUT_BLOCK;  // sites per layout block
 __host__ __device__ __forceinline__ size_t padded_sites(size_t V) { return (V + LAYOUT_BLOCK - 1) / LAYOUT_BLOCK * LAYOUT_BLOCK; }
 // offset of complex entry k of link mu at site s; entry k+1 is LAYOUT_BLOCK further
 __host__ __device__ __forceinline__ size_t link_offset(int mu, int k, int s) {
