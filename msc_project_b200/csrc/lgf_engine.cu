@@ -216,7 +216,7 @@ public:
         LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rk3_stage<R, 1>, threads_, 0));
         stage_grid_max_ = std::max(1, nb) * ctx_->sm_count;
         LGF_CUDA_TRY(ctx_, prepare_measure_kernel<R>());
-        LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R>, MEAS_SITES * 6,
+        LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R>, MEAS_SITES * MEAS_WARPS,
                                                                          measure_smem_bytes<R>()));
         meas_grid_max_ = std::max(1, nb) * ctx_->sm_count;
         if (dynamic_) {
@@ -354,7 +354,7 @@ public:
             if (k == 1) k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
             if (k == 2) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
         } else {
-            k_measure<R><<<meas_grid(), dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+            k_measure<R><<<meas_grid(), dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R>(), ctx_->stream>>>(
                 d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
         }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
@@ -365,7 +365,7 @@ public:
         const int mg = meas_grid();
         const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
         const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
-        k_measure<R><<<mg, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+        k_measure<R><<<mg, dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R>(), ctx_->stream>>>(
             d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
         k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
         k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
@@ -640,7 +640,7 @@ template <typename R> static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf
     if (e == cudaSuccess) e = cudaMemcpyAsync(dmt, mt.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        k_measure<R, true><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, 6), measure_smem_bytes<R, true>(),
+        k_measure<R, true><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R, true>(),
                              ctx->stream>>>((const LatDesc<R>*)ddesc, dmt, dn, out);
         e = cudaGetLastError();
     }

@@ -32,11 +32,14 @@
 #ifndef LGF_STAGE_MINB
 #define LGF_STAGE_MINB 1
 #endif
+#ifndef LGF_MEAS_QSPLIT
+#define LGF_MEAS_QSPLIT 2  // measurement warps per plane (the four quadrants split between them)
+#endif
 #ifndef LGF_MEAS_MINB_D
-#define LGF_MEAS_MINB_D 2  // double: resident measurement blocks per SM (caps registers)
+#define LGF_MEAS_MINB_D (LGF_MEAS_QSPLIT == 2 ? 1 : 2)  // double: resident measurement blocks per SM (caps registers)
 #endif
 #ifndef LGF_MEAS_MINB_F
-#define LGF_MEAS_MINB_F 2  // float
+#define LGF_MEAS_MINB_F (LGF_MEAS_QSPLIT == 2 ? 1 : 2)  // float
 #endif
 
 namespace lgf {
@@ -289,12 +292,20 @@ __device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
 __device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
 
 constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
+constexpr int MEAS_QSPLIT = LGF_MEAS_QSPLIT;
+constexpr int MEAS_WARPS = 6 * MEAS_QSPLIT;  // warp y: plane y % 6, quadrants of part y / 6
 
 // Shared memory of one measurement block: the straight lines of length 2 and
 // 3 from each of its 32 sites in the 8 signed directions (every plane and
 // quadrant of the site reuses them), then the per-plane results.
 template <typename R, bool OUT> struct MeasSmem {
-    R line[8][2][18][MEAS_SITES];     // [2*dir + (sign<0)][length-2][entry][site]
+    union {
+        R line[8][2][18][MEAS_SITES];  // [2*dir + (sign<0)][length-2][entry][site]
+        struct {                       // after the lines are dead: the second quadrant half's sums
+            alg<R> G[6][MEAS_SITES];
+            alg<R> Fh[6][MEAS_SITES];
+        } part;
+    };
     alg<R> F[6][MEAS_SITES];          // improved F per plane
     alg<R> C[OUT ? 6 : 1][MEAS_SITES];  // clover F per plane (single-lattice passes only)
     double E[6][MEAS_SITES];
@@ -330,13 +341,15 @@ __device__ __forceinline__ su3<R> load_line(const MeasSmem<R, OUT>* sm, int sdir
     return L;
 }
 
-// Clover F and improved F of plane (mu, nu) at the thread's site, using the
+// Quadrants [qa, qb) of plane (mu, nu) at the thread's site, using the
 // block's shared lines (21 matrix products and 16 global link loads per
-// quadrant).  See the comment above Plane for the leaf decomposition.
+// quadrant): G = the sum of the 1x1 leaves' projections, Fhat = the weighted
+// sum of the other shapes' (see the comment above Plane for the leaf
+// decomposition).  The clover F is G/4 and the improved F is Fhat + 19/36 G.
 template <typename R, bool OUT>
 __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
-                                                  int mu, int nu, const MeasSmem<R, OUT>* sm, int lane, alg<R>& F11,
-                                                  alg<R>& Fhat) {
+                                                  int mu, int nu, const MeasSmem<R, OUT>* sm, int lane, int qa, int qb,
+                                                  alg<R>& G, alg<R>& Fhat) {
     Plane<R> P;
     P.U = U;
     P.V = g.V;
@@ -345,15 +358,14 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
     P.dm = dir_of(g, c, mu);
     P.dn = dir_of(g, c, nu);
     const PlanePos x0 = {s, P.dm.x, P.dn.x};
-    const R k11 = R(19.0 / 36.0), k12 = R(-4.0 / 45.0), k13 = R(1.0 / 120.0), k22 = R(1.0 / 144.0);
-    alg<R> G;
+    const R k12 = R(-4.0 / 45.0), k13 = R(1.0 / 120.0), k22 = R(1.0 / 144.0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         G.v[k] = R(0);
         Fhat.v[k] = R(0);
     }
 #pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
+    for (int q = qa; q < qb; ++q) {
         const int sm_ = (q == 0 || q == 1) ? 1 : -1;
         const int sn = (q == 0 || q == 2) ? 1 : -1;
         const R sg = (q == 0 || q == 3) ? R(1) : R(-1);
@@ -417,17 +429,15 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
             leaf_acc(Pn, Pm, sg * k22, Fhat);
         }
     }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        F11.v[k] = R(0.25) * G.v[k];
-        Fhat.v[k] = fma(k11, G.v[k], Fhat.v[k]);
-    }
 }
 
 // Measurement tile = (lattice, x0 slice, chunk of 32 consecutive sites of the
-// slice); 6 warps = 6 planes.  Phase 0: the block's lines (warp w builds the
-// lines of signed direction w, and w+6 for w < 2) into shared memory.  Phase
-// 1: F and F^ of every (site, plane).  Phase 2: the six planes meet in shared
+// slice); 6 x MEAS_QSPLIT warps: warp y takes plane y % 6 and the quadrants
+// of part y / 6.  Phase 0: the block's lines (warp w builds the lines of
+// signed direction w, w + MEAS_WARPS, ...) into shared memory.  Phase 1: the
+// quadrant sums of every (site, plane); with two parts the second part's sums
+// meet the first's in the (then dead) line storage, in a fixed order, for F
+// and F^.  Phase 2: the six planes meet in shared
 // memory for e(x) and q(x); the tile's sums go to the lattice's
 // partial[slice * nchunk + chunk] (double2).  The optional outputs of
 // MeasOut (single-lattice passes) receive per-site densities and per
@@ -440,13 +450,14 @@ template <typename R> struct MeasMinBlocks { static constexpr int value = LGF_ME
 template <> struct MeasMinBlocks<double> { static constexpr int value = LGF_MEAS_MINB_D; };
 
 template <typename R, bool OUT = false>
-__global__ void __launch_bounds__(MEAS_SITES * 6, MeasMinBlocks<R>::value) k_measure(const LatDesc<R>* __restrict__ descs,
+__global__ void __launch_bounds__(MEAS_SITES * MEAS_WARPS, MeasMinBlocks<R>::value) k_measure(const LatDesc<R>* __restrict__ descs,
                                                                            const int4* __restrict__ mtiles,
                                                                            const int* __restrict__ nmtiles,
                                                                            MeasOut out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MeasSmem<R, OUT>* sm = reinterpret_cast<MeasSmem<R, OUT>*>(smem_raw);
-    const int lane = threadIdx.x, p = threadIdx.y;
+    const int lane = threadIdx.x, w = threadIdx.y, p = w % 6, part = w / 6;
+    const int qa = part * (4 / MEAS_QSPLIT), qb = qa + 4 / MEAS_QSPLIT;
     const int n = *nmtiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
         const int4 tile = mtiles[ti];
@@ -459,7 +470,7 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, MeasMinBlocks<R>::value) k_mea
         const Coord c = site_coord(g, s);
         const cplx<R>* __restrict__ U = d->U0;
         // phase 0: lines of length 2 and 3 in the 8 signed directions
-        for (int sdir = p; sdir < 8; sdir += 6) {
+        for (int sdir = w; sdir < 8; sdir += MEAS_WARPS) {
             const int dir = sdir >> 1, sign = (sdir & 1) ? -1 : 1;
             Plane<R> L;
             L.U = U;
@@ -476,10 +487,32 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, MeasMinBlocks<R>::value) k_mea
             store_line(sm, sdir, 3, lane, acc);
         }
         __syncthreads();
-        // phase 1: this thread's plane
-        if (valid) {
-            alg<R> F11, Fh;
-            plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, F11, Fh);
+        // phase 1: this thread's plane and quadrants
+        alg<R> G, Fh;
+        if (valid) plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, qa, qb, G, Fh);
+        if (MEAS_QSPLIT == 2) {
+            __syncthreads();  // every warp is done with the lines
+            if (part == 1 && valid) {
+                sm->part.G[p][lane] = G;
+                sm->part.Fh[p][lane] = Fh;
+            }
+            __syncthreads();
+            if (part == 0 && valid) {
+                const alg<R> G1 = sm->part.G[p][lane], F1 = sm->part.Fh[p][lane];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    G.v[k] += G1.v[k];
+                    Fh.v[k] += F1.v[k];
+                }
+            }
+        }
+        if (part == 0 && valid) {
+            alg<R> F11;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                F11.v[k] = R(0.25) * G.v[k];
+                Fh.v[k] = fma(R(19.0 / 36.0), G.v[k], Fh.v[k]);
+            }
             sm->F[p][lane] = Fh;
             sm->E[p][lane] = retr_hh(F11, F11);
             if (OUT) {
@@ -490,7 +523,7 @@ __global__ void __launch_bounds__(MEAS_SITES * 6, MeasMinBlocks<R>::value) k_mea
         }
         __syncthreads();
         // phase 2: the site's e(x), q(x) and the tile's sums
-        if (p == 0) {
+        if (w == 0) {
             double e = 0.0, q = 0.0;
             if (valid) {
                 e = ((sm->E[0][lane] + sm->E[1][lane]) + (sm->E[2][lane] + sm->E[3][lane])) +
