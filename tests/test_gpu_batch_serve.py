@@ -30,6 +30,8 @@ def mixed_jobs():
         Job((6, 6, 6, 12), FP64, seed=102, nsteps=10, meas_every=5, want_links=True),
         Job((8, 8, 8, 8), FP32MIXED, seed=103, nsteps=12, meas_every=3, reunit_every=5, want_links=True),
         Job((4, 8, 8, 8), FP32MIXED, seed=104, nsteps=5, meas_every=5, want_links=True),
+        Job((6, 6, 6, 6), FP64, seed=105, nsteps=6, meas_every=3, want_links=True),  # V = 1296: not a whole number of 32-site blocks
+        Job((6, 6, 6, 6), FP32MIXED, seed=106, nsteps=6, meas_every=3, reunit_every=3, want_links=True),
     ]
 
 

@@ -329,3 +329,30 @@ def test_invalid_arguments(ctx):
     with ctx.lattice((4, 4, 4, 4), FP64) as lat:
         with pytest.raises(ValueError):
             lat.upload(np.zeros(10))
+
+
+def test_unaligned_volume_against_oracle(ctx):
+    """V = 6^4 = 1296 sites is not a whole number of the device layout's
+    32-site blocks: the padded tail must never leak into links, E or Q."""
+    shape = (6, 6, 6, 6)
+    U = O.generate_G(shape, 21, 0.5)
+    t, E, Q, Uo = O.flow(U, shape, 0.01, 6, 2)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        assert np.array_equal(lat.download(), U)
+        r = lat.flow(0.01, 6, 2, slices=True)
+        Ug = lat.download()
+        e, q = lat.site_densities()
+        u, d = lat.unitarity()
+    assert rel_err(r.E, E) < 1e-12 and q_err(r.Q, Q) < 1e-12
+    assert np.max(np.abs(Ug - Uo)) < TOL
+    assert np.allclose(r.E_slice.mean(axis=1), r.E, rtol=1e-13)
+    eo, qo = O.site_densities(Uo, shape)
+    assert np.max(np.abs(e - eo)) < 1e-12 and np.max(np.abs(q - qo)) < 1e-12
+    assert u < 1e-13 and d < 1e-13
+    with ctx.lattice(shape, FP64) as lat:
+        lat.hot_start(4)
+        lat.heatbath(6.0, 2, 1, seed=5)
+        p1 = lat.plaquette()
+        lat.overrelax(3)
+        assert abs(lat.plaquette() - p1) < 1e-13
