@@ -799,10 +799,11 @@ int lgf_flow(lgf_lattice* lat, const lgf_flow_opts* o, lgf_meas* out) {
             return set_error(ctx, LGF_EINVAL, "result capacity %d < %d measurements", out->capacity, nmeas);
     }
     cudaSetDevice(ctx->device);
+    const double* meas_before = lat->buf.meas;
     int rc = buf_grow_meas(ctx, lat->buf, nmeas);
     if (rc != LGF_OK) return rc;
-    if (lat->group && lat->buf.meas_cap > 0) {
-        // the measurement buffer may have moved: refresh the descriptor
+    if (lat->group && lat->buf.meas != meas_before) {
+        // the measurement buffer moved: refresh the descriptor
         std::vector<LatticeBuf*> m{&lat->buf};
         rc = lat->group->set_members(m);
         if (rc != LGF_OK) return rc;
