@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -37,7 +38,7 @@ struct ServeJob {
     size_t bytes = 0;
     LatticeBuf buf;
     int nmeas = 0;
-    int steps_done = 0;
+    std::atomic<int> steps_done{0};  // advanced by the worker, read by pollers
     double t = 0.0;
     std::vector<double> tvals;
 };
@@ -53,7 +54,8 @@ struct lgf_server {
     lgf_serve_config cfg{};
     std::chrono::steady_clock::time_point t0;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_idle;
+    int waiters = 0;  // threads inside lgf_serve_wait; stop frees the server only when none is left
     std::deque<ServeJob*> queue;
     std::map<uint64_t, std::unique_ptr<ServeJob>> jobs;
     std::vector<ServeJob*> active;
@@ -325,12 +327,14 @@ int lgf_serve_wait(lgf_server* s, uint64_t id, double timeout_s, lgf_job_status*
     if (it == s->jobs.end()) return LGF_ENOTFOUND;
     ServeJob* j = it->second.get();
     auto done = [&] { return j->st.state == LGF_JOB_DONE || j->st.state == LGF_JOB_FAILED; };
-    if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(std::max(timeout_s, 0.0)), done)) {
-        if (st) *st = j->st;
-        return LGF_ETIMEDOUT;
+    ++s->waiters;
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(std::max(timeout_s, 0.0)), done);
+    if (st) {
+        *st = j->st;
+        st->steps_done = j->steps_done;
     }
-    if (st) *st = j->st;
-    return LGF_OK;
+    if (--s->waiters == 0) s->cv_idle.notify_all();
+    return ok ? LGF_OK : LGF_ETIMEDOUT;
 }
 
 int lgf_serve_stop(lgf_server* s) {
@@ -347,7 +351,13 @@ int lgf_serve_stop(lgf_server* s) {
         s->cv_work.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
-    s->cv_done.notify_all();
+    {
+        // every job has ended by now; let threads blocked in lgf_serve_wait
+        // return before the server is freed
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.notify_all();
+        s->cv_idle.wait(lk, [s] { return s->waiters == 0; });
+    }
     delete s;
     return LGF_OK;
 }

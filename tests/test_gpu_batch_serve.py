@@ -84,3 +84,32 @@ def test_server_rejects_jobs_that_never_fit(ctx):
         assert e.value.code == C.LGF_EINVAL
         rc, _ = srv.poll(12345)
         assert rc == C.LGF_ENOTFOUND
+
+
+def test_server_stop_while_threads_wait(ctx):
+    """lgf_serve_stop while other threads block in lgf_serve_wait (one on the
+    running job, one on a queued job): both waits return with the job ended
+    by LGF_ESHUTDOWN, and the server is freed only after they have left."""
+    import ctypes
+    import threading
+    srv = Server(ctx, 1 << 34, max_active=1, steps_per_tick=1)
+    ids = [srv.submit(Job((16, 16, 16, 16), FP64, seed=2, nsteps=50000, measure_at_t0=False)),
+           srv.submit(Job((8, 8, 8, 8), FP64, seed=3, nsteps=10, measure_at_t0=False))]
+    results = {}
+
+    def waiter(jid):
+        st = C.lgf_job_status()
+        rc = ctx.lib.lgf_serve_wait(srv.h, ctypes.c_uint64(jid), 120.0, ctypes.byref(st))
+        results[jid] = (rc, st.state, st.error)
+
+    threads = [threading.Thread(target=waiter, args=(i,)) for i in ids]
+    for t in threads:
+        t.start()
+    time.sleep(1.0)  # both waiters are blocked inside lgf_serve_wait
+    assert not results
+    srv.stop()
+    for t in threads:
+        t.join(30.0)
+        assert not t.is_alive()
+    for jid in ids:
+        assert results[jid] == (C.LGF_OK, C.LGF_JOB_FAILED, C.LGF_ESHUTDOWN)
