@@ -114,8 +114,9 @@ bool save_links(SimulationParameters& p, const std::string& method, const std::s
         std::cout << LGF_EIO << " Error: cannot open " << path << std::endl;
         return false;
     }
-    const bool ok = std::fwrite(links.data(), sizeof(double), links.size(), f) == links.size();
-    std::fclose(f);
+    bool ok = std::fwrite(links.data(), sizeof(double), links.size(), f) == links.size();
+    ok = (std::fclose(f) == 0) && ok;  // a failed flush is a failed save
+    if (!ok) std::cout << LGF_EIO << " Error: cannot write " << path << std::endl;
     return ok;
 }
 
@@ -320,7 +321,7 @@ static int qdensity_impl(SimulationParameters& params, FlowParameters& fp) {
         std::FILE* f = std::fopen(out.string().c_str(), "r+b");
         if (!f) f = std::fopen(out.string().c_str(), "w+b");
         if (!f || std::fwrite(q.data(), sizeof(double), q.size(), f) != q.size()) status = LGF_EIO;
-        if (f) std::fclose(f);
+        if (f && std::fclose(f) != 0) status = LGF_EIO;
     }
     return status;
 }
