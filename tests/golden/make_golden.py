@@ -74,6 +74,32 @@ def reference_flow(work: Path, links: np.ndarray, shape, steps, eps, meas):
     return E, Q, csv_e, csv_q, files[0].name if files else None, flowed
 
 
+def reference_resume(work: Path, out: Path):
+    """ResumeFlowedConfiguration (LGF/LGF.cpp:197-226) on the flow above: pick
+    up the saved t = 1.0 configuration, 50 more steps measuring every 5; the
+    reference appends to the same CSV files and saves the t = 1.5 links."""
+    shape = (8, 8, 8, 8)
+    r = run_ref(["resume", str(work) + "/", "6.0", *shape, 0, 0, 50, 0.01, 5, "1.0"])
+    E, Q = parse_stdout(r.stdout)
+    obs = work / "Observables"
+    csv_q = (obs / "Topological_Charge" / BETA_DIR / shape_dir(shape) / "GF" / "torus_extdof4_0.csv").read_text()
+    csv_e = (obs / "EnergyDensity" / BETA_DIR / shape_dir(shape) / "GF" / "torus_extdof4_0.csv").read_text()
+    f = work / "ensembles" / "su3" / BETA_DIR / shape_dir(shape) / "GF" / "torus_extdof4_0_Flowtime1.500000.bin"
+    flowed = np.fromfile(f)
+    t, tv = 1.0, []
+    for s in range(1, 51):
+        t += 0.01
+        if s % 5 == 0:
+            tv.append(t)
+    rec = {"shape": list(shape), "beta": 6.0, "eps": 0.01, "steps": 50, "meas_every": 5, "t_pickup": 1.0,
+           "input": "the t = 1.0 links of flow8_hb_seed1.json", "t": tv, "E": E, "Q": Q,
+           "csv_energy": csv_e, "csv_topcharge": csv_q, "flowed_file": f.name,
+           "flowed_sha256": hashlib.sha256(flowed.tobytes()).hexdigest(),
+           "flowed_sample": flowed[: 4 * 18 * 2].tolist(),
+           "generator": "oracle/_ref/lgf_ref (unmodified LGF sources) via tests/golden/make_golden.py"}
+    out.write_text(json.dumps(rec, indent=1))
+
+
 def times(n_meas, eps, meas):
     t, out = 0.0, [0.0]
     for s in range(1, (n_meas - 1) * meas + 1):
@@ -116,6 +142,7 @@ def main():
         links = np.fromfile(hb)
         res = reference_flow(tmp / "f8", links, (8, 8, 8, 8), 100, 0.01, 1)
         write_flow_json(HERE / "flow8_hb_seed1.json", (8, 8, 8, 8), 100, 0.01, 1, hb.name, *res)
+        reference_resume(tmp / "f8", HERE / "resume8_hb_seed1.json")
 
         # ---- small generator-G lattice: per-function outputs and a short flow
         shape = (4, 4, 6, 6)

@@ -356,3 +356,34 @@ def test_unaligned_volume_against_oracle(ctx):
         p1 = lat.plaquette()
         lat.overrelax(3)
         assert abs(lat.plaquette() - p1) < 1e-13
+
+
+def test_resume_against_reference(ctx, tmp_path):
+    """The reference's own ResumeFlowedConfiguration (LGF.cpp:197-226) run on
+    its config-1 flow: pick up t = 1.0, 50 steps measuring every 5.  The
+    drop-in's appended CSV files are byte-identical, E(t)/Q(t) agree to 1e-12
+    and the saved t = 1.5 links to 1e-11."""
+    from msc_project_b200 import (FlowParameters, FlowSavedGaugeConfigurations, ResumeFlowedConfiguration,
+                                  SimulationParameters, configure)
+    g = golden_json("resume8_hb_seed1.json")
+    configure(FP64)
+    folder = str(tmp_path) + "/"
+    d = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/LHMC_3_of_0_330000"
+    d.mkdir(parents=True)
+    (d / "torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
+    p = SimulationParameters(4, 4, [8, 8, 8, 8], 6.0, [0, 0, 0, 0])
+    assert FlowSavedGaugeConfigurations(p, FlowParameters(0, 0, 100, 0.01, 1, folder)) == 0
+    gf = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/GF"
+    U1 = np.fromfile(gf / "torus_extdof4_0_Flowtime1.000000.bin")
+    assert ResumeFlowedConfiguration(p, FlowParameters(0, 0, 50, 0.01, 5, folder), 1.0) == 0
+    obs = tmp_path / "Observables"
+    assert (obs / "EnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text() == g["csv_energy"]
+    assert (obs / "Topological_Charge/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text() == g["csv_topcharge"]
+    Uf = np.fromfile(gf / g["flowed_file"])
+    assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < 1e-11
+    with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+        lat.upload(U1)
+        r = lat.flow(0.01, 50, 5, t0=1.0, measure_at_t0=False)
+    assert np.array_equal(r.t, np.array(g["t"]))
+    assert rel_err(r.E, g["E"]) < 1e-12
+    assert q_err(r.Q, g["Q"]) < 1e-12

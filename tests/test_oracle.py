@@ -68,3 +68,19 @@ def test_oracle_flow_16():
     assert rel_err(E, g["E"]) < 1e-12
     assert q_err(Q, g["Q"]) < 1e-12
     assert hashlib.sha256(Uf.tobytes()).hexdigest() == g["flowed_sha256"]
+
+
+def test_oracle_resume_against_reference():
+    """Continuing the oracle's t = 1.0 links (byte-identical to the reference's)
+    for 50 steps reproduces the reference's ResumeFlowedConfiguration: E/Q at
+    every measurement and the saved t = 1.5 file byte for byte."""
+    g8 = golden_json("flow8_hb_seed1.json")
+    g = golden_json("resume8_hb_seed1.json")
+    U = golden_links("hb8_seed1.bin")
+    _, _, _, U1 = O.flow(U, (8, 8, 8, 8), 0.01, 100, 0)
+    assert hashlib.sha256(U1.tobytes()).hexdigest() == g8["flowed_sha256"]
+    t, E, Q, U2 = O.flow(U1, (8, 8, 8, 8), 0.01, 50, 5, 1.0)
+    assert np.array_equal(t[1:], np.array(g["t"]))  # the reference does not measure at the pickup time
+    assert rel_err(E[1:], g["E"]) < 1e-12
+    assert q_err(Q[1:], g["Q"]) < 1e-12
+    assert hashlib.sha256(U2.tobytes()).hexdigest() == g["flowed_sha256"]
