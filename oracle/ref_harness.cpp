@@ -14,6 +14,9 @@
 //   resume <folder> <beta> <N0> <N1> <N2> <N3> <start> <stop> <steps> <eps> <meas> <t_pickup>
 //       ResumeFlowedConfiguration(params, flowParams, t_pickup) (LGF/LGF.cpp:197-226)
 //       from <folder>'s saved <cfg>_Flowtime<t_pickup> file, std::cout as above.
+//   qdensity|measureflowed <folder> <beta> <N0> <N1> <N2> <N3> <start> <stop> <steps> <eps> <meas>
+//       MeasureQdensityDistribution / MeasureFlowedGaugeConfigurations
+//       (LGF/LGF.cpp:113-123, :228-255) on the saved <cfg>_Flowtime<eps*steps> files.
 //   kernels <links.bin> <N0> <N1> <N2> <N3> <out_prefix>
 //       per-function outputs in global site order: staple (SU3_field.cpp:519),
 //       flow gradient (Wilson.cpp:55), clover F (SU3_field.cpp:533),
@@ -213,7 +216,7 @@ int cmd_cpubench(int argc, char** argv) {
 int main(int argc, char** argv) {
     mpiWrapper::begin_parallelSession(argc, argv);
     if (argc < 2) {
-        std::fprintf(stderr, "usage: lgf_ref heatbath|flow|resume|kernels|exp|cpubench ...\n");
+        std::fprintf(stderr, "usage: lgf_ref heatbath|flow|resume|qdensity|measureflowed|kernels|exp|cpubench ...\n");
         return 2;
     }
     std::string cmd = argv[1];
@@ -240,6 +243,19 @@ int main(int argc, char** argv) {
                           std::atoi(argv[12]), argv[2]);
         std::cout << std::setprecision(17);
         ResumeFlowedConfiguration(params, fp, std::stod(argv[13]));
+        rc = 0;
+    } else if ((cmd == "qdensity" || cmd == "measureflowed") && argc >= 13) {
+        // MeasureQdensityDistribution (LGF.cpp:113-123) / MeasureFlowedGaugeConfigurations
+        // (LGF.cpp:228-255) on <folder>'s saved <cfg>_Flowtime<eps*steps> files
+        std::vector<int> shape = shape_from(argv + 4);
+        SimulationParameters params(4, 4, shape, std::stod(argv[3]), {0, 0, 0, 0}, "torus");
+        FlowParameters fp(std::atoi(argv[8]), std::atoi(argv[9]), std::atoi(argv[10]), std::stod(argv[11]),
+                          std::atoi(argv[12]), argv[2]);
+        std::cout << std::setprecision(17);
+        if (cmd == "qdensity")
+            MeasureQdensityDistribution(params, fp);
+        else
+            MeasureFlowedGaugeConfigurations(params, fp);
         rc = 0;
     } else if (cmd == "kernels") {
         rc = cmd_kernels(argc - 1, argv + 1);

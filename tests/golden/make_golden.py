@@ -100,6 +100,36 @@ def reference_resume(work: Path, out: Path):
     out.write_text(json.dumps(rec, indent=1))
 
 
+def reference_measure_workflows(tmp: Path, out_json: Path, out_q: Path):
+    """The reference's MeasureQdensityDistribution and
+    MeasureFlowedGaugeConfigurations (LGF/LGF.cpp:113-123, :228-255) on the
+    config-1 flow's saved t = 1.0 links (FlowParameters(0, 0, 100, 0.01, 1)),
+    each in a fresh folder holding only that file."""
+    shape = (8, 8, 8, 8)
+    rel = Path("ensembles") / "su3" / BETA_DIR / shape_dir(shape) / "GF"
+    src = tmp / "f8" / rel / "torus_extdof4_0_Flowtime1.000000.bin"
+    res = {}
+    for cmd in ("qdensity", "measureflowed"):
+        d = tmp / cmd
+        (d / rel).mkdir(parents=True)
+        shutil.copy(src, d / rel / src.name)
+        res[cmd] = run_ref([cmd, str(d) + "/", "6.0", *shape, 0, 0, 100, 0.01, 1])
+    q = np.fromfile(tmp / "qdensity" / "Observables" / "Qdensity" / BETA_DIR / shape_dir(shape) / "GF" /
+                    "torus_extdof1_0_Flowtime1.000000.bin")
+    q.tofile(out_q)
+    E, Q = parse_stdout(res["measureflowed"].stdout)
+    obs = tmp / "measureflowed" / "Observables"
+    rec = {"shape": list(shape), "beta": 6.0, "flow_time": 1.0, "input": "the t = 1.0 links of flow8_hb_seed1.json",
+           "E_improved": E, "Q_clover": Q,
+           "csv_energy": (obs / "ImprovedEnergyDensity" / BETA_DIR / shape_dir(shape) / "GF" /
+                          "torus_extdof4_0.csv").read_text(),
+           "csv_topcharge": (obs / "UnImprovedTopological_Charge" / BETA_DIR / shape_dir(shape) / "GF" /
+                             "torus_extdof4_0.csv").read_text(),
+           "qdensity_file": out_q.name, "qdensity_sha256": hashlib.sha256(q.tobytes()).hexdigest(),
+           "generator": "oracle/_ref/lgf_ref (unmodified LGF sources) via tests/golden/make_golden.py"}
+    out_json.write_text(json.dumps(rec, indent=1))
+
+
 def times(n_meas, eps, meas):
     t, out = 0.0, [0.0]
     for s in range(1, (n_meas - 1) * meas + 1):
@@ -143,6 +173,7 @@ def main():
         res = reference_flow(tmp / "f8", links, (8, 8, 8, 8), 100, 0.01, 1)
         write_flow_json(HERE / "flow8_hb_seed1.json", (8, 8, 8, 8), 100, 0.01, 1, hb.name, *res)
         reference_resume(tmp / "f8", HERE / "resume8_hb_seed1.json")
+        reference_measure_workflows(tmp, HERE / "measure8_t1.json", HERE / "qdensity8_t1.bin")
 
         # ---- small generator-G lattice: per-function outputs and a short flow
         shape = (4, 4, 6, 6)

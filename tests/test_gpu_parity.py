@@ -387,3 +387,40 @@ def test_resume_against_reference(ctx, tmp_path):
     assert np.array_equal(r.t, np.array(g["t"]))
     assert rel_err(r.E, g["E"]) < 1e-12
     assert q_err(r.Q, g["Q"]) < 1e-12
+
+
+def test_measure_workflows_against_reference(ctx, tmp_path):
+    """The reference's own MeasureFlowedGaugeConfigurations and
+    MeasureQdensityDistribution (LGF.cpp:228-255, :113-123) on its config-1
+    t = 1.0 links: improved E and clover Q to 1e-12 with byte-identical CSV
+    files, and the q-density file (with its pi^2/4 prefactor) to 1e-12."""
+    from msc_project_b200 import (FlowParameters, FlowSavedGaugeConfigurations, MeasureFlowedGaugeConfigurations,
+                                  MeasureQdensityDistribution, SimulationParameters, configure)
+    g = golden_json("measure8_t1.json")
+    qref = np.fromfile(GOLDEN / g["qdensity_file"])
+    configure(FP64)
+    p = SimulationParameters(4, 4, [8, 8, 8, 8], 6.0, [0, 0, 0, 0])
+    rel = "ensembles/su3/beta6_000000/8X8X8X8"
+    src = tmp_path / "flow"
+    (src / rel / "LHMC_3_of_0_330000").mkdir(parents=True)
+    (src / rel / "LHMC_3_of_0_330000/torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
+    assert FlowSavedGaugeConfigurations(p, FlowParameters(0, 0, 100, 0.01, 1, str(src) + "/")) == 0
+    U1 = (src / rel / "GF/torus_extdof4_0_Flowtime1.000000.bin").read_bytes()
+    for name in ("measure", "qdensity"):
+        (tmp_path / name / rel / "GF").mkdir(parents=True)
+        (tmp_path / name / rel / "GF/torus_extdof4_0_Flowtime1.000000.bin").write_bytes(U1)
+    fp = lambda name: FlowParameters(0, 0, 100, 0.01, 1, str(tmp_path / name) + "/")  # noqa: E731
+    assert MeasureFlowedGaugeConfigurations(p, fp("measure")) == 0
+    assert MeasureQdensityDistribution(p, fp("qdensity")) == 0
+    obs = tmp_path / "measure/Observables"
+    assert (obs / "ImprovedEnergyDensity/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text() == g["csv_energy"]
+    assert (obs / "UnImprovedTopological_Charge/beta6_000000/8X8X8X8/GF/torus_extdof4_0.csv").read_text() == \
+        g["csv_topcharge"]
+    q = np.fromfile(tmp_path / "qdensity/Observables/Qdensity/beta6_000000/8X8X8X8/GF/"
+                    "torus_extdof1_0_Flowtime1.000000.bin")
+    assert q.shape == qref.shape and np.max(np.abs(q - qref)) < 1e-12
+    with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+        lat.upload(np.frombuffer(U1, dtype=np.float64))
+        Ei, Qc = lat.measure_flowed()
+    assert abs(Ei - g["E_improved"][0]) < 1e-12 * abs(g["E_improved"][0])
+    assert abs(Qc - g["Q_clover"][0]) < 1e-12 * max(1.0, abs(g["Q_clover"][0]))

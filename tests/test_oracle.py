@@ -84,3 +84,14 @@ def test_oracle_resume_against_reference():
     assert rel_err(E[1:], g["E"]) < 1e-12
     assert q_err(Q[1:], g["Q"]) < 1e-12
     assert hashlib.sha256(U2.tobytes()).hexdigest() == g["flowed_sha256"]
+
+
+def test_oracle_qdensity_against_reference():
+    """The oracle's per-site q(x) on its t = 1.0 links (byte-identical to the
+    reference's) times the reference's pi^2/4 prefactor equals the q-density
+    file the reference's MeasureQdensityDistribution wrote."""
+    g = golden_json("measure8_t1.json")
+    qref = np.fromfile(GOLDEN / g["qdensity_file"])
+    _, _, _, U1 = O.flow(golden_links("hb8_seed1.bin"), (8, 8, 8, 8), 0.01, 100, 0)
+    _, q = O.site_densities(U1, (8, 8, 8, 8))
+    assert np.max(np.abs((np.pi ** 2 / 4) * q - qref)) < 1e-13
