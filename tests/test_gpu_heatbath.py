@@ -104,3 +104,27 @@ def test_dropin_generate_heatbath_files(ctx, tmp_path):
     # continuing an ensemble loads configuration `start` (LGF.cpp:146-148)
     assert GenerateHeatBathGaugeConfigurations(p, HBParameters(2, 3, 0, 2, 5, folder), seed=4) == 0
     assert (d / "torus_extdof4_3.bin").exists()
+
+
+def test_heatbath_ensemble_matches_the_reference(ctx):
+    """Statistical parity with the reference's own heatbath ensemble (nine
+    configurations, seeds 1..9, 200 x (CM + 5 OR) at beta 6.0 on 8^4): twelve
+    GPU chains give the same mean plaquette and mean E, |Q| after flowing to
+    t = 1.0, within three standard errors of the difference.  The GPU chains
+    are reproducible by seed, so the check is deterministic."""
+    from conftest import golden_json
+    g = golden_json("hb8_ensemble.json")
+    ref = {k: np.array([c[k] for c in g["configs"]]) for k in ("plaquette", "E_t1", "Q_t1")}
+    gpu = {k: [] for k in ref}
+    for i in range(12):
+        with ctx.lattice((8, 8, 8, 8), FP64) as lat:
+            lat.hot_start(200 + i)
+            assert lat.heatbath(6.0, 200, 5, seed=300 + i) <= 10
+            gpu["plaquette"].append(lat.plaquette())
+            r = lat.flow(0.01, 100, 100)
+            gpu["E_t1"].append(r.E[-1])
+            gpu["Q_t1"].append(r.Q[-1])
+    for k, f in (("plaquette", lambda x: x), ("E_t1", lambda x: x), ("Q_t1", np.abs)):
+        a, b = f(np.array(gpu[k])), f(ref[k])
+        se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
+        assert abs(a.mean() - b.mean()) < 3 * se, (k, a.mean(), b.mean(), se)
