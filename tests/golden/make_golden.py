@@ -192,6 +192,13 @@ def main():
         res = reference_flow(tmp / "fg", g, shape, 20, 0.01, 5)
         write_flow_json(HERE / "flow_g4466.json", shape, 20, 0.01, 5, "g4466_seed7.bin", *res)
 
+        # ---- four different extents (every axis distinguishable), generator G seed 9
+        shape = (4, 6, 8, 10)
+        g4 = O.generate_G(shape, 9, 0.5)
+        g4.tofile(tmp / "g46810.bin")
+        res = reference_flow(tmp / "f46810", g4, shape, 20, 0.01, 4)
+        write_flow_json(HERE / "flow_g46810.json", shape, 20, 0.01, 4, "generator G seed 9 scale 0.5", *res)
+
         # ---- exponential on both Cayley-Hamilton branches
         rng = np.random.default_rng(2024)
         n = 512

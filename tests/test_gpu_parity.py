@@ -424,3 +424,21 @@ def test_measure_workflows_against_reference(ctx, tmp_path):
         Ei, Qc = lat.measure_flowed()
     assert abs(Ei - g["E_improved"][0]) < 1e-12 * abs(g["E_improved"][0])
     assert abs(Qc - g["Q_clover"][0]) < 1e-12 * max(1.0, abs(g["Q_clover"][0]))
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32MIXED])
+def test_flow_four_extents_against_reference(ctx, prec):
+    """Every axis of a different length (4, 6, 8, 10), generator G seed 9:
+    the reference's E(t), Q(t) and flowed links (FP64 to 1e-12; the FP32-mixed
+    form within its accuracy gates)."""
+    g = golden_json("flow_g46810.json")
+    U = O.generate_G(g["shape"], 9, 0.5)
+    with ctx.lattice(g["shape"], prec) as lat:
+        lat.upload(U)
+        r = lat.flow(g["eps"], g["steps"], g["meas_every"], reunit_every=10 if prec == FP32MIXED else 0)
+        Uf = lat.download()
+    tol = TOL if prec == FP64 else 1e-5
+    assert np.allclose(r.t, g["t"], rtol=0, atol=1e-12)
+    assert rel_err(r.E, g["E"]) < tol
+    assert q_err(r.Q, g["Q"]) < (TOL if prec == FP64 else 1e-3)
+    assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < (TOL if prec == FP64 else 1e-5)

@@ -95,3 +95,13 @@ def test_oracle_qdensity_against_reference():
     _, _, _, U1 = O.flow(golden_links("hb8_seed1.bin"), (8, 8, 8, 8), 0.01, 100, 0)
     _, q = O.site_densities(U1, (8, 8, 8, 8))
     assert np.max(np.abs((np.pi ** 2 / 4) * q - qref)) < 1e-13
+
+
+def test_oracle_flow_four_extents():
+    """Every axis of a different length (4, 6, 8, 10): E/Q and the flowed file
+    match the reference's, so no two directions are mixed up."""
+    g = golden_json("flow_g46810.json")
+    U = O.generate_G(g["shape"], 9, 0.5)
+    t, E, Q, Uf = O.flow(U, g["shape"], g["eps"], g["steps"], g["meas_every"])
+    assert rel_err(E, g["E"]) < 1e-12 and q_err(Q, g["Q"]) < 1e-12
+    assert hashlib.sha256(Uf.tobytes()).hexdigest() == g["flowed_sha256"]
