@@ -442,3 +442,21 @@ def test_flow_four_extents_against_reference(ctx, prec):
     assert rel_err(r.E, g["E"]) < tol
     assert q_err(r.Q, g["Q"]) < (TOL if prec == FP64 else 1e-3)
     assert np.max(np.abs(Uf[: len(g["flowed_sample"])] - np.array(g["flowed_sample"]))) < (TOL if prec == FP64 else 1e-5)
+
+
+def test_long_flow_against_oracle(ctx):
+    """500 RK3 steps (t = 5) of the config-1 input: the flow is contracting,
+    so the GPU and the oracle stay together to rounding over a long flow
+    (E, Q every 100 steps and the final links)."""
+    shape = (8, 8, 8, 8)
+    U = golden_links("hb8_seed1.bin")
+    t, E, Q, Uo = O.flow(U, shape, 0.01, 500, 100)
+    with ctx.lattice(shape, FP64) as lat:
+        lat.upload(U)
+        r = lat.flow(0.01, 500, 100)
+        Ug = lat.download()
+        u, d = lat.unitarity()
+    assert np.array_equal(r.t, t)
+    assert rel_err(r.E, E) < 1e-12 and q_err(r.Q, Q) < 1e-12
+    assert np.max(np.abs(Ug - Uo)) < 1e-12
+    assert u < 1e-13 and d < 1e-13
