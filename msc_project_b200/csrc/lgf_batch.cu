@@ -47,10 +47,14 @@ int validate_job(lgf_ctx* ctx, const lgf_job& j) {
 
 int tune_threads(lgf_ctx* ctx, int prec, const int shape[4], int* best);
 
+// block size for a wave whose largest lattice has this shape: tuned once per
+// precision and volume class (a small lattice prefers more, smaller blocks)
 int threads_for(lgf_ctx* ctx, int prec, const int shape[4]) {
-    if (ctx->tuned_threads[prec]) return ctx->tuned_threads[prec];
+    const long long V = 1LL * shape[0] * shape[1] * shape[2] * shape[3];
+    for (const auto& t : ctx->tuned)
+        if (t.prec == prec && V <= 2 * t.volume && t.volume <= 2 * V) return t.threads;
     int best = default_threads(prec);
-    if (tune_threads(ctx, prec, shape, &best) == LGF_OK) ctx->tuned_threads[prec] = best;
+    if (tune_threads(ctx, prec, shape, &best) == LGF_OK) record_tuned(ctx, prec, V, best);
     return best;
 }
 
@@ -239,7 +243,7 @@ int lgf_autotune(lgf_ctx* ctx, int precision, const int shape[4], int* best_thre
     int best = 0;
     int rc = tune_threads(ctx, precision, shape, &best);
     if (rc != LGF_OK) return rc;
-    ctx->tuned_threads[precision] = best;
+    record_tuned(ctx, precision, 1LL * shape[0] * shape[1] * shape[2] * shape[3], best);
     if (best_threads) *best_threads = best;
     return LGF_OK;
 }

@@ -16,7 +16,10 @@ struct lgf_ctx {
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     std::string err;
-    int tuned_threads[2] = {0, 0};  // per precision; 0 = not tuned yet
+    // autotuned stage block sizes: (precision, lattice volume, threads); a
+    // result applies to volumes within a factor of two of the tuned one
+    struct Tuned { int prec; long long volume; int threads; };
+    std::vector<Tuned> tuned;
     // two pinned host chunks for uploads/downloads from pageable memory
     // (allocated on first use; a server's worker shares them, hence the lock)
     void* pin[2] = {nullptr, nullptr};
@@ -38,6 +41,9 @@ int set_error(lgf_ctx* ctx, int code, const char* fmt, ...);
 bool valid_shape(const int shape[4]);
 size_t footprint_bytes(const int shape[4], int precision, int meas_slots);
 int default_threads(int precision);
+// the tuned block size for a lattice of this precision and volume, else the default
+int stage_threads(const lgf_ctx* ctx, int precision, long long volume);
+void record_tuned(lgf_ctx* ctx, int precision, long long volume, int threads);
 
 // Device resources of one lattice (precision-erased).
 struct LatticeBuf {

@@ -271,7 +271,7 @@ int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out)
     if (s->cfg.steps_per_tick < 1) s->cfg.steps_per_tick = 1;
     s->t0 = std::chrono::steady_clock::now();
     for (int p = 0; p < 2; ++p) {
-        s->threads[p] = ctx->tuned_threads[p] ? ctx->tuned_threads[p] : default_threads(p);
+        s->threads[p] = default_threads(p);  // jobs of every volume share the server's launches
         // the budget bounds the resident sites: every site costs at least its links ring + accumulator
         const size_t per_site = (p == 0 ? 8 : 4) * (3 * 4 * 18 + 4 * 8);
         const long long max_sites = (long long)(cfg->hbm_budget_bytes / per_site) + 1;
