@@ -203,6 +203,31 @@ static void append_stage_tiles(std::vector<int2>& tiles, int i, const Geom& g, i
             }
 }
 
+#ifndef LGF_STAGE_ORDER
+#define LGF_STAGE_ORDER 1  // stage tile order: 0 blocks of x1 rows swept through x0, 1 x1 columns per CTA
+#endif
+// Column order: a column is the tiles at one (x0, position in the x1 row) for
+// x1 = 0..N1-1.  Columns are taken G at a time (G = the persistent grid) and
+// listed row by row, so CTA b walks column b along x1: the x1 - 1 neighbours
+// of its tile are the links of the tile it did before.  Needs tiles that lie
+// inside one x1 row (N2 N3 a multiple of T) and bands of G columns that span
+// at least 8 x0 slices (else most x0 neighbours fall on a band edge: 48^4
+// with 64-site tiles spans 4); returns false otherwise.  Measured against the
+// blocked order: +3-4% flow-only on 24^3x48 and 32^4.
+static bool append_stage_tiles_columns(std::vector<int2>& tiles, int i, const Geom& g, int T, int G) {
+    const long long row = (long long)g.n[2] * g.n[3];
+    if (row % T || G < 1) return false;
+    const long long per_row = row / T, ncol = g.n[0] * per_row;
+    if (8 * per_row > G && ncol > G) return false;
+    for (long long c0 = 0; c0 < ncol; c0 += G) {
+        const long long c1 = std::min(c0 + (long long)G, ncol);
+        for (long long x1 = 0; x1 < g.n[1]; ++x1)
+            for (long long c = c0; c < c1; ++c)
+                tiles.push_back(make_int2(i, (int)((c / per_row) * g.Vs + x1 * row + (c % per_row) * T)));
+    }
+    return true;
+}
+
 // measurement tiles (lattice, slice, 32-site chunk of the slice) of lattice i
 static void append_measure_tiles(std::vector<int4>& tiles, int i, const Geom& g, double bytes_per_site) {
     const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
@@ -279,7 +304,8 @@ public:
             d.eps = (R)b.eps;
             // a tile is threads_/4 consecutive sites with all four link directions;
             // per site a stage reads and writes 4 links and 4 su(3) accumulators
-            append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, 4.0 * (2 * 18 + 8) * sizeof(R));
+            if (!(LGF_STAGE_ORDER == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
+                append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, 4.0 * (2 * 18 + 8) * sizeof(R));
             mt += (long long)b.g.n[0] * b.nchunk;
         }
         if ((long long)tiles.size() > max_tiles_)
