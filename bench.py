@@ -18,8 +18,10 @@ sweep of arrival rates, and heatbath generation.
 
 --impl reference runs the LGF reference itself (oracle/_ref/lgf_ref, the
 unmodified sources) on the host cores: one single-rank process per core,
-each flowing an 8^4 sample with the same schedule (10 RK3 steps + one E/Q
-measurement per chunk); value = processes * V * 10 / chunk time.
+each flowing a 16^4 sample of the generator input (per-site cost as on
+24^3x48: both exceed the host caches), RK3 steps and one E/Q measurement
+timed apart; value = processes * V * 300 / (300 step times + 31 measurement
+times), the bench job's schedule.
 
 --gpus N (under torchrun) runs N independent replicas, one per GPU ("replicas
 only": the flow of one lattice does not shard); value sums all ranks' work
@@ -57,6 +59,7 @@ FLOPS_PER_SITE_STAGE = 42888.0 / 3
 # dram__bytes_write.sum), scaled to this workload; see profiles/.
 NCU_STAGE_TRAFFIC_BYTES = {0: 1135.0e6, 1: 548.4e6}  # stage-2 launch; profiles/k_rk3_stage_*_24x24x24x48.md
 FP64_FMA_PER_SM_PER_CLK = 64  # B200: 64 FP64 FMA lanes per SM (nominal)
+FP32_FMA_PER_SM_PER_CLK = 128  # B200: 128 FP32 FMA lanes per SM (nominal)
 N_SM = 148
 
 
@@ -153,31 +156,56 @@ def barrier(dist):
 
 
 # --------------------------------------------------------------- reference
-def run_reference_sample(nproc: int, chunks: int, warm: int):
-    """nproc single-rank reference processes in parallel, each flowing the 8^4
-    config-1 input for `chunks` chunks of 10 RK3 steps + 1 measurement."""
+# The reference's per-site cost on lattices that exceed the host's caches is
+# volume-independent (16^4 and 24^3x48 both stream their fields from DRAM),
+# so each host core flows a 16^4 sample of the bench's generator input; the
+# full 24^3x48 lattice costs ~45 s per RK3 step on one core (REF_SAMPLE_SHAPE
+# can be set to it with --ref-shape).
+REF_SAMPLE_SHAPE = (16, 16, 16, 16)
+
+
+def run_reference_sample(nproc: int, steps: int, warm: int, shape=REF_SAMPLE_SHAPE):
+    """nproc single-rank reference processes in parallel (oracle/_ref/lgf_ref
+    cpusplit: the unmodified GradientFlow/observable code), each flowing the
+    generator-G (seed 7) configuration of `shape` for `steps` RK3 steps timed
+    one by one, then one E/Q measurement.  The rate applies the bench job's
+    schedule (NSTEPS steps, a measurement at t=0 and every MEAS steps) to the
+    slowest process's median step and measurement times."""
+    import tempfile
+
     from oracle import oracle as O
     if not O.reference_available():
         return None, "oracle/_ref/lgf_ref not built"
-    inp = ROOT / "tests" / "golden" / "hb8_seed1.bin"
+    V = int(shape[0] * shape[1] * shape[2] * shape[3])
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = Path(tmp) / "g7.bin"
+        O.generate_G(shape, SEED, 0.5).tofile(inp)
 
-    def one(_):
-        out = O.run_reference(["cpubench", inp, 8, 8, 8, 8, MEAS * chunks, MEAS], timeout=1800)
-        line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
-        return json.loads(line)
+        def one(_):
+            out = O.run_reference(["cpusplit", inp, *shape, steps], timeout=3600)
+            line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
+            return json.loads(line)
 
-    with ThreadPoolExecutor(max_workers=nproc) as ex:
-        res = list(ex.map(one, range(nproc)))
-    # per chunk: the slowest process defines the aggregate rate
-    per_chunk = [max(r["chunks_s"][c] for r in res) for c in range(warm, chunks)]
-    V = 8 ** 4
-    rates = [nproc * V * MEAS / t for t in per_chunk]
-    return {"value": statistics.median(rates), "per_chunk_s": per_chunk, "cores": nproc,
+        with ThreadPoolExecutor(max_workers=nproc) as ex:
+            res = list(ex.map(one, range(nproc)))
+    per_step = [max(r["step_s"][i] for r in res) for i in range(warm, steps)]
+    meas_s = max(r["measure_s"] for r in res)
+    t_step = statistics.median(per_step)
+    nmeas = 1 + NSTEPS // MEAS
+    job_s = NSTEPS * t_step + nmeas * meas_s  # one process's job on the sample lattice
+    value = nproc * V * NSTEPS / job_s
+    return {"value": value, "per_step_s": per_step, "measure_s": meas_s, "cores": nproc,
+            "flow_only": nproc * V / t_step,
             "lattice_setup_s": max(r["setup_s"] for r in res),
-            "sample": f"{nproc} parallel single-rank reference processes, 8^4 heatbath config (seed 1), "
-                      f"{chunks} chunks of 10 RK3 steps + 1 E/Q measurement each, first {warm} chunks untimed; "
-                      f"the reference's Lattice/field setup and input read (lattice_setup_s) is outside the timed "
-                      f"chunks"}, None
+            "sample": f"{nproc} parallel single-rank reference processes (no MPI on the host), each the "
+                      f"{'x'.join(map(str, shape))} generator-G seed-7 configuration: {steps} RK3 steps timed one by "
+                      f"one (first {warm} untimed) and one E/Q measurement; rate = the bench job's schedule "
+                      f"({NSTEPS} steps + {nmeas} measurements) at the slowest process's median step and "
+                      f"measurement times; the Lattice/field setup and input read (lattice_setup_s) is excluded"}, None
+
+
+def _ref_shape(args):
+    return tuple(int(x) for x in args.ref_shape.split(",")) if args.ref_shape else REF_SAMPLE_SHAPE
 
 
 def reference_arm(args):
@@ -185,7 +213,8 @@ def reference_arm(args):
     if rank != 0:
         return
     nproc = args.ref_procs or os.cpu_count() or 1
-    res, err = run_reference_sample(nproc, args.warmup + args.steps, args.warmup)
+    shape = _ref_shape(args)
+    res, err = run_reference_sample(nproc, args.warmup + args.steps, args.warmup, shape)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
@@ -193,11 +222,13 @@ def reference_arm(args):
         "impl": "reference",
         "metric": "site-RK3-steps/s", "value": res["value"], "unit": "site-RK3-steps/s",
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * statistics.median(res["per_chunk_s"]),
+        "ms_per_step": 1e3 * statistics.median(res["per_step_s"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "reference_sample": "8^4 per process"},
+        "config": {"workload": WORKLOAD, "reference_sample": f"{'x'.join(map(str, shape))} per process",
+                   "step": "one RK3 step of every process (wall, slowest process); one E/Q measurement after them"},
         "cpu_baseline": {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"],
-                         "kind": "reference", "sample": res["sample"], "lattice_setup_s": res["lattice_setup_s"]},
+                         "kind": "reference", "sample": res["sample"], "measure_s": res["measure_s"],
+                         "flow_only": res["flow_only"], "lattice_setup_s": res["lattice_setup_s"]},
         "e2e": {"value": res["value"], "unit": "site-RK3-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -446,15 +477,18 @@ def engine_arm(args):
     achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
     clocks = clk.summary()
     mhz = clocks["sm_mhz"] or 1965.0
-    fma_peak = N_SM * FP64_FMA_PER_SM_PER_CLK * 2 * mhz * 1e6 / 1e12
+    pipe_name = "fp64" if prec == FP64 else "fp32"
+    fma_lanes = FP64_FMA_PER_SM_PER_CLK if prec == FP64 else FP32_FMA_PER_SM_PER_CLK
+    fma_peak = N_SM * fma_lanes * 2 * mhz * 1e6 / 1e12
     stage_tflops = V * FLOPS_PER_SITE_STAGE / (stage_ms * 1e-3) / 1e12
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res, err = run_reference_sample(args.ref_procs or os.cpu_count() or 1, 3, 1)
+        res, err = run_reference_sample(args.ref_procs or os.cpu_count() or 1, 3, 1, _ref_shape(args))
         if res:
             cpu = {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"], "kind": "reference",
-                   "sample": res["sample"], "lattice_setup_s": res["lattice_setup_s"]}
+                   "sample": res["sample"], "measure_s": res["measure_s"], "flow_only": res["flow_only"],
+                   "lattice_setup_s": res["lattice_setup_s"]}
         else:
             cpu = {"value": None, "unavailable": err}
 
@@ -481,14 +515,23 @@ def engine_arm(args):
                 "d2h_bytes_per_step": nmeas * 3 * 8},
         "flow_only": {"value": flow_only, "unit": "site-RK3-steps/s",
                       "note": "the same 300 steps without E/Q measurements (device time)"},
-        "roofline": {"bound": "hbm", "binding": f"fp64 FMA pipe (fp64_pipe below): one stage is "
-                     f"{V * FLOPS_PER_SITE_STAGE / (fma_peak * 1e12) * 1e3:.3f} ms of FP64 FMA work at peak and "
-                     f"{stage_bytes / (hbm_peak * 1e9) * 1e3:.3f} ms of HBM traffic at the measured copy rate",
-                     "kernel": "k_rk3_stage (mean of the 3 stages)", "achieved": achieved,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": NCU_STAGE_TRAFFIC_BYTES[prec], "traffic_note": "DRAM bytes of one stage-2 launch (ncu), algorithmic 1104 MB (FP64) / 552 MB (FP32)", "stage_ms": stage_ms, "measure_ms": ms[3]},
-        "fp64_pipe": {"achieved_tflops": stage_tflops, "nominal_peak_tflops_at_clock": fma_peak,
-                      "frac": stage_tflops / fma_peak, "note": "canonical flops / stage time vs 148 SM x 64 FP64 FMA x 2 x median SM clock"},
+        "roofline": {"bound": pipe_name, "kernel": "k_rk3_stage (mean of the 3 stages)",
+                     "achieved": stage_tflops, "peak": fma_peak, "unit": "TFLOP/s", "frac": stage_tflops / fma_peak,
+                     "peak_kind": f"nominal: {N_SM} SM x {fma_lanes} {pipe_name.upper()} FMA lanes x 2 flops x the run's "
+                                  f"median SM clock (no measured {pipe_name.upper()} peak exists for this pool)",
+                     "binding": f"{pipe_name} FMA pipe: one stage is "
+                                f"{V * FLOPS_PER_SITE_STAGE / (fma_peak * 1e12) * 1e3:.3f} ms of FMA work at the nominal "
+                                f"peak and {stage_bytes / (hbm_peak * 1e9) * 1e3:.3f} ms of HBM traffic at the measured "
+                                f"copy rate",
+                     "flops_per_launch": V * FLOPS_PER_SITE_STAGE,
+                     "traffic": NCU_STAGE_TRAFFIC_BYTES[prec],
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-2 launch on this "
+                                       "workload (profiles/k_rk3_stage_*), a constant carried from that capture, not "
+                                       "re-measured by this run",
+                     "algorithmic_bytes": stage_bytes,
+                     "hbm": {"achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                             "peak_kind": peak_kind},
+                     "stage_ms": stage_ms, "measure_ms": ms[3]},
         "cpu_baseline": cpu,
         "forms": forms,
         "clocks": clocks,
@@ -526,6 +569,8 @@ def main():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--precision", choices=["fp64", "fp32mixed"], default="fp64")
     ap.add_argument("--ref-procs", type=int, default=0)
+    ap.add_argument("--ref-shape", default="", help="lattice of the reference's per-process sample, e.g. 48,24,24,24 "
+                                                    "(default 16,16,16,16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the forms (volumes, FP32-mixed, batched, served, heatbath)")
     ap.add_argument("--forms", default="all", help="comma list of forms to run (default all)")

@@ -145,10 +145,15 @@ int lgf_last_flow_seconds(lgf_lattice* lat, double* seconds);
  * The launches are asynchronous on that stream; out is valid once it completes.
  * Scratch is a fixed device array inside the library (4 MiB + 4 KiB per GPU,
  * held until exit): N0 <= 256 and N0 * ceil(N1*N2*N3/32) <= 262144 (48^4 fits,
- * 64^4 does not); larger lattices return LGF_ETOOBIG.  The first call on a
- * device looks up the array's device address, so make it before any stream
- * capture.  Calls share the array: calls that may overlap on one GPU (other
- * streams, other host threads) race and must be ordered by the caller. */
+ * 64^4 does not); larger lattices return LGF_ETOOBIG.  CUDA loads a module
+ * (and with it this array) lazily by default: the array's device address is
+ * looked up -- which loads it -- by lgf_ctx_create on that device, or else by
+ * the first lgf_measure_noalloc call there.  Make one of the two before
+ * reserving the rest of the GPU's memory and before any stream capture.
+ * An error left pending by earlier work on the calling thread is not
+ * cleared: the call then returns LGF_ECUDA without launching.  Calls share
+ * the array: calls that may overlap on one GPU (other streams, other host
+ * threads) race and must be ordered by the caller. */
 int lgf_measure_noalloc(const double* links, const int shape[4], double* out, void* stream);
 
 /* ------------------------------------------------------- configurations */

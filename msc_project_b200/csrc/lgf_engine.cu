@@ -389,9 +389,18 @@ public:
     int launch_step() override {
         if (!dynamic_ && ntiles_ == 0) return LGF_OK;
         const int grid = stage_grid();
-        k_rk3_stage<R, 1><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-        k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-        k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
+        {
+            NvtxRange r("lgf.rk3_stage1");
+            k_rk3_stage<R, 1><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
+        }
+        {
+            NvtxRange r("lgf.rk3_stage2");
+            k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
+        }
+        {
+            NvtxRange r("lgf.rk3_stage3");
+            k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
+        }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
     }
@@ -412,6 +421,7 @@ public:
     }
 
     int launch_measure() override {
+        NvtxRange r("lgf.measure_launch");
         const int mg = meas_grid();
         const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
         const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
@@ -437,6 +447,7 @@ public:
         return capture_one(false, &meas_exec_);
     }
     int replay_step() override {
+        NvtxRange r("lgf.rk3_step");
         if (!step_exec_) {
             int rc = capture();
             if (rc != LGF_OK) return rc;
@@ -445,6 +456,7 @@ public:
         return LGF_OK;
     }
     int replay_measure() override {
+        NvtxRange r("lgf.measure");
         if (!meas_exec_) {
             int rc = capture();
             if (rc != LGF_OK) return rc;
@@ -513,22 +525,25 @@ GroupBase* make_group(lgf_ctx* ctx, int precision, int threads, int max_members,
 // ----------------------------------------------------------- link movement
 static inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
+// one block per 32-site layout block (the transpose kernels above)
 int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file) {
     const int V = b.g.V;
+    const int nb = blocks_for(V, LAYOUT_BLOCK);
     if (b.prec == LGF_PREC_FP64)
-        k_to_device<double><<<blocks_for(4LL * V, 256), 256, 0, ctx->stream>>>((const double2*)dev_file, (cplx<double>*)b.U[0], V);
+        k_to_device<double><<<nb, CONV_THREADS, 0, ctx->stream>>>((const double2*)dev_file, (cplx<double>*)b.U[0], V);
     else
-        k_to_device<float><<<blocks_for(4LL * V, 256), 256, 0, ctx->stream>>>((const double2*)dev_file, (cplx<float>*)b.U[0], V);
+        k_to_device<float><<<nb, CONV_THREADS, 0, ctx->stream>>>((const double2*)dev_file, (cplx<float>*)b.U[0], V);
     LGF_CUDA_TRY(ctx, cudaGetLastError());
     return LGF_OK;
 }
 
 int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file) {
     const int V = b.g.V;
+    const int nb = blocks_for(V, LAYOUT_BLOCK);
     if (b.prec == LGF_PREC_FP64)
-        k_to_file<double><<<blocks_for(4LL * V, 256), 256, 0, ctx->stream>>>((const cplx<double>*)b.U[0], (double2*)dev_file, V);
+        k_to_file<double><<<nb, CONV_THREADS, 0, ctx->stream>>>((const cplx<double>*)b.U[0], (double2*)dev_file, V);
     else
-        k_to_file<float><<<blocks_for(4LL * V, 256), 256, 0, ctx->stream>>>((const cplx<float>*)b.U[0], (double2*)dev_file, V);
+        k_to_file<float><<<nb, CONV_THREADS, 0, ctx->stream>>>((const cplx<float>*)b.U[0], (double2*)dev_file, V);
     LGF_CUDA_TRY(ctx, cudaGetLastError());
     return LGF_OK;
 }
@@ -731,6 +746,13 @@ int lgf_ctx_create(int device, lgf_ctx** out) {
         delete ctx;
         return LGF_ECUDA;
     }
+    // place lgf_measure_noalloc's fixed scratch now, before the caller's own
+    // allocations (modules load lazily otherwise)
+    if (noalloc_preload(device) != LGF_OK) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return LGF_ECUDA;
+    }
     *out = ctx;
     return LGF_OK;
 }
@@ -849,6 +871,7 @@ int lgf_flow(lgf_lattice* lat, const lgf_flow_opts* o, lgf_meas* out) {
             return set_error(ctx, LGF_EINVAL, "result capacity %d < %d measurements", out->capacity, nmeas);
     }
     cudaSetDevice(ctx->device);
+    NvtxRange flow_range("lgf.flow");
     const double* meas_before = lat->buf.meas;
     int rc = buf_grow_meas(ctx, lat->buf, nmeas);
     if (rc != LGF_OK) return rc;

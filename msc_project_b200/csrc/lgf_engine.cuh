@@ -11,6 +11,23 @@
 #include "../../include/lgf_b200.h"
 #include "lgf_kernels.cuh"
 
+// NVTX ranges around the host-side launch points (RK3 steps, stages,
+// measurements), visible on an Nsight timeline; header-only NVTX is a no-op
+// unless a tool is attached.  -DLGF_NO_NVTX compiles them out.
+#ifndef LGF_NO_NVTX
+#include <nvtx3/nvToolsExt.h>
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#else
+struct NvtxRange {
+    explicit NvtxRange(const char*) {}
+};
+#endif
+
 struct lgf_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -100,6 +117,10 @@ void release_pinned_chunks(lgf_ctx* ctx);
 
 // measurement schedule of FlowSavedGaugeConfigurations for one job
 int count_measurements(const lgf_flow_opts& o);
+
+// loads lgf_measure_noalloc's module (and scratch array) on device dev, which
+// must be current (lgf_noalloc.cu)
+int noalloc_preload(int dev);
 
 }  // namespace lgf
 

@@ -643,30 +643,53 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_total(const LatDesc<R>* 
 }
 
 // ------------------------------------------------------------- layouts
-// file order (double, [s][mu][k][re,im]) -> device layout in precision R
+// File order (double, [s][mu][k][re,im]) <-> device layout in precision R.
+// The 32 sites of one layout block occupy one contiguous run in both orders
+// (file: 32 x 36 complex, site-major; device: 36 x 32 complex, entry-major),
+// so a block of CONV_THREADS threads moves one layout block as a transpose
+// through shared memory: both the global read and the global write are
+// consecutive 16-byte (or 8-byte) words across the warp.  Sites past V in
+// the last block are neither read nor written.
+constexpr int CONV_THREADS = 256;
+constexpr int CONV_PITCH = 37;  // 36 entries + 1: columns of the transpose hit distinct banks
+
 template <typename R>
-__global__ void k_to_device(const double2* __restrict__ file, cplx<R>* __restrict__ U, int V) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * V) return;
-    const int mu = t / V, s = t - mu * V;
-    const double2* src = file + ((size_t)s * 4 + mu) * 9;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const double2 v = src[k];
-        U[link_offset(mu, k, s)] = cmk<R>((R)v.x, (R)v.y);
+__global__ void __launch_bounds__(CONV_THREADS) k_to_device(const double2* __restrict__ file, cplx<R>* __restrict__ U,
+                                                            int V) {
+    __shared__ double2 t[LAYOUT_BLOCK * CONV_PITCH];
+    const int b = blockIdx.x;
+    const int s0 = b * LAYOUT_BLOCK;
+    const int ns = min(LAYOUT_BLOCK, V - s0);
+    const double2* src = file + (size_t)s0 * 36;
+    for (int i = threadIdx.x; i < ns * 36; i += CONV_THREADS) t[(i / 36) * CONV_PITCH + i % 36] = src[i];
+    __syncthreads();
+    cplx<R>* dst = U + (size_t)b * 36 * LAYOUT_BLOCK;
+    for (int j = threadIdx.x; j < 36 * LAYOUT_BLOCK; j += CONV_THREADS) {
+        const int e = j / LAYOUT_BLOCK, site = j % LAYOUT_BLOCK;
+        if (site < ns) {
+            const double2 v = t[site * CONV_PITCH + e];
+            stc(dst + j, cmk<R>((R)v.x, (R)v.y));
+        }
     }
 }
 template <typename R>
-__global__ void k_to_file(const cplx<R>* __restrict__ U, double2* __restrict__ file, int V) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * V) return;
-    const int mu = t / V, s = t - mu * V;
-    double2* dst = file + ((size_t)s * 4 + mu) * 9;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const cplx<R> z = U[link_offset(mu, k, s)];
-        dst[k] = make_double2((double)z.re, (double)z.im);
+__global__ void __launch_bounds__(CONV_THREADS) k_to_file(const cplx<R>* __restrict__ U, double2* __restrict__ file,
+                                                          int V) {
+    __shared__ double2 t[LAYOUT_BLOCK * CONV_PITCH];
+    const int b = blockIdx.x;
+    const int s0 = b * LAYOUT_BLOCK;
+    const int ns = min(LAYOUT_BLOCK, V - s0);
+    const cplx<R>* src = U + (size_t)b * 36 * LAYOUT_BLOCK;
+    for (int j = threadIdx.x; j < 36 * LAYOUT_BLOCK; j += CONV_THREADS) {
+        const int e = j / LAYOUT_BLOCK, site = j % LAYOUT_BLOCK;
+        if (site < ns) {
+            const cplx<R> z = ldc(src + j);
+            t[site * CONV_PITCH + e] = make_double2((double)z.re, (double)z.im);
+        }
     }
+    __syncthreads();
+    double2* dst = file + (size_t)s0 * 36;
+    for (int i = threadIdx.x; i < ns * 36; i += CONV_THREADS) dst[i] = t[(i / 36) * CONV_PITCH + i % 36];
 }
 
 // --------------------------------------------------------- generator G

@@ -12,13 +12,17 @@
 // The scratch array is a host-side symbol: host code must not pass its name
 // to a kernel (that would hand the kernel a host address).  Its device address
 // is looked up once per device with cudaGetSymbolAddress, with that device
-// current, on the first call made on that device; that first call should
-// therefore come before any stream capture.  Every GPU that loads the library
-// holds the array (4 MiB + 4 KiB) until the process exits.  All calls on one
-// GPU share it and it keeps the last call's contents: two calls that can run
-// at the same time on the same GPU (different streams, different host
-// threads) race on it, so the caller must order them.  Nothing in it has to
-// start at zero: each call writes every entry it later reads.
+// current.  CUDA loads modules lazily by default, so that lookup is also what
+// places the array in the GPU's memory: lgf_ctx_create does it for its device
+// (noalloc_preload), and otherwise the first call made on a device does it.
+// Callers that reserve the rest of the GPU's memory must therefore create a
+// context or make one call first, and the first call should come before any
+// stream capture.  Once loaded, a GPU holds the array (4 MiB + 4 KiB) until
+// the process exits.  All calls on one GPU share it and it keeps the last
+// call's contents: two calls that can run at the same time on the same GPU
+// (different streams, different host threads) race on it, so the caller must
+// order them.  Nothing in it has to start at zero: each call writes every
+// entry it later reads.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -208,7 +212,7 @@ int noalloc_scratch(int dev, double2** out) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
-            cudaGetLastError();
+            if (e != cudaSuccess) cudaGetLastError();  // this lookup's own error
             return LGF_ECUDA;
         }
         g_noalloc_addr[dev] = (double2*)p;
@@ -218,6 +222,16 @@ int noalloc_scratch(int dev, double2** out) {
 }
 
 }  // namespace
+
+// Called by lgf_ctx_create with the context's device current: loads this
+// file's module on that device (placing the scratch array) and caches its
+// address, so the first measurement allocates nothing even under lazy loading.
+int noalloc_preload(int dev) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return LGF_OK;  // such devices are served on first call
+    double2* p = nullptr;
+    return noalloc_scratch(dev, &p);
+}
+
 }  // namespace lgf
 
 extern "C" int lgf_measure_noalloc(const double* links, const int shape[4], double* out, void* stream) {
@@ -227,11 +241,11 @@ extern "C" int lgf_measure_noalloc(const double* links, const int shape[4], doub
     const int nchunk = (g.Vs + MEAS_SITES - 1) / MEAS_SITES;
     if (g.n[0] > NOALLOC_MAX_SLICES || (long long)nchunk * g.n[0] > NOALLOC_MAX_PARTIALS) return LGF_ETOOBIG;
     if (((uintptr_t)links % 16) != 0 || ((uintptr_t)out % 8) != 0) return LGF_EINVAL;
+    // an error that earlier work left pending on this thread is the caller's:
+    // report it without clearing it, and launch nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return LGF_ECUDA;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
-        cudaGetLastError();
-        return LGF_ECUDA;
-    }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return LGF_ECUDA;
     double2* scratch = nullptr;
     int rc = noalloc_scratch(dev, &scratch);
     if (rc != LGF_OK) return rc;
@@ -241,6 +255,7 @@ extern "C" int lgf_measure_noalloc(const double* links, const int shape[4], doub
     k_noalloc_measure<<<dim3(nchunk, g.n[0]), dim3(MEAS_SITES, 6), 0, st>>>((const double2*)links, g, partials);
     k_noalloc_slices<<<g.n[0], RED_THREADS, 0, st>>>(partials, nchunk, g, slice_sums, out);
     k_noalloc_total<<<1, RED_THREADS, 0, st>>>(slice_sums, g, out);
+    // nothing was pending at entry, so an error now comes from these launches
     if (cudaGetLastError() != cudaSuccess) return LGF_ECUDA;
     return LGF_OK;
 }

@@ -27,10 +27,15 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
 
-def build() -> None:
-    """Compile the oracle restatement (and the reference harness where the
-    reference tree exists) with oracle/Makefile."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+def build(ref_dir: str | os.PathLike | None = None) -> None:
+    """Compile the oracle restatement with oracle/Makefile, and the reference
+    harness too when ``ref_dir`` (or the environment variable LGF_REFERENCE)
+    names the reference's ``LGF/`` source directory."""
+    ref = ref_dir if ref_dir is not None else os.environ.get("LGF_REFERENCE")
+    cmd = ["make", "-s", "-C", str(HERE)]
+    if ref and (Path(ref) / "LGF.cpp").exists():
+        cmd.append(f"REF={Path(ref).resolve()}")
+    subprocess.run(cmd, check=True)
 
 
 _lib = None

@@ -28,6 +28,10 @@
 //   cpubench <links.bin|hot> <N0> <N1> <N2> <N3> <steps> <meas_every>
 //       the hot loop of FlowSavedGaugeConfigurations (LGF.cpp:166-188) without
 //       file output, timed; prints one JSON line.
+//   cpusplit <links.bin|hot> <N0> <N1> <N2> <N3> <steps>
+//       the same objects, timed apart: each of <steps> GradientFlow::flow()
+//       calls (no measurement falls due), then one GradientFlow::MakeMeasurements()
+//       (Q then E, GradientFlow.cpp:76-83); prints one JSON line.
 #include "LGF.h"
 
 #include <chrono>
@@ -211,6 +215,50 @@ int cmd_cpubench(int argc, char** argv) {
     return 0;
 }
 
+int cmd_cpusplit(int argc, char** argv) {
+    if (argc < 7) return 2;
+    std::string in = argv[1];
+    std::vector<int> shape = shape_from(argv + 2);
+    int steps = std::atoi(argv[6]);
+    auto t0 = std::chrono::steady_clock::now();
+    SimulationParameters params(4, 4, shape, 6.0, {0, 0, 0, 0}, "torus");
+    Lattice lattice(params, true);
+    Wilson action(params.getbeta());
+    SU3_field U(lattice, params.getextdofs());
+    if (in == "hot") {
+        U.InitializeHotStart();
+    } else if (!load_raw(U, lattice, in)) {
+        std::fprintf(stderr, "cannot read %s\n", in.c_str());
+        return 3;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    std::streambuf* saved = std::cout.rdbuf();
+    std::ostringstream sink;
+    std::cout.rdbuf(sink.rdbuf());
+    // measurement interval beyond the step count: flow() never measures here
+    GradientFlow flowing(action, U, 0.01, steps + 1);
+    TopologicalCharge topCharge(U);
+    flowing.Include_TopCharge(topCharge);
+    EnergyDensity Edensity(U);
+    flowing.Include_EnergyDensity(Edensity);
+    std::vector<double> step_s;
+    for (int i = 0; i < steps; i++) {
+        auto a = std::chrono::steady_clock::now();
+        flowing.flow();
+        step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count());
+    }
+    auto m0 = std::chrono::steady_clock::now();
+    flowing.MakeMeasurements();
+    const double meas_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - m0).count();
+    std::cout.rdbuf(saved);
+    long long V = (long long)shape[0] * shape[1] * shape[2] * shape[3];
+    std::printf("{\"sites\": %lld, \"steps\": %d, \"setup_s\": %.6f, \"measure_s\": %.6f, \"step_s\": [", V, steps,
+                std::chrono::duration<double>(t1 - t0).count(), meas_s);
+    for (size_t i = 0; i < step_s.size(); ++i) std::printf(i ? ", %.6f" : "%.6f", step_s[i]);
+    std::printf("]}\n");
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -263,6 +311,8 @@ int main(int argc, char** argv) {
         rc = cmd_exp(argc - 1, argv + 1);
     } else if (cmd == "cpubench") {
         rc = cmd_cpubench(argc - 1, argv + 1);
+    } else if (cmd == "cpusplit") {
+        rc = cmd_cpusplit(argc - 1, argv + 1);
     }
     mpiWrapper::end_parallelSession();
     return rc;

@@ -17,15 +17,26 @@ oracle/Makefile with the single-rank MPI stub and the seed shim) and writes:
   flow_g4466.json          FlowSavedGaugeConfigurations on it: 20 steps, meas every 5
   exp_cases.npz            HermTrLessExp on 512 matrices spanning both branches
   flow16_g7.json           16^4 generator-G seed 7: 10 steps, measure every 5
+  flow16_g7_t3.json        16^4 generator-G seed 7 as the throughput
+                           configuration runs it: eps=0.01 to t=3.0 (300 steps),
+                           E/Q at t=0 and every 10 steps, CSVs, and the flowed
+                           links' SHA-256 plus 32 sampled sites
+  flow24x48_g7.json        24^3x48 generator-G seed 7 (the bench lattice, x0 = 48):
+                           3 steps measuring every 3 (t=0 and t=0.03), flowed
+                           links' SHA-256 plus 32 sampled sites
 
-Usage:  python tests/golden/make_golden.py [--skip-heatbath] [--skip-16]
-The heatbath takes ~3 min and the 8^4 flow ~1.5 min on one core.
+Usage:  python tests/golden/make_golden.py [--reference DIR] [--skip-heatbath] [--skip-16]
+                                          [--only small|t3|bench]
+The heatbath takes ~3 min and the 8^4 flow ~1.5 min on one core; flow16_g7_t3
+about 40 min and flow24x48_g7 about 10 min (--only t3 / --only bench make
+just those).
 """
 from __future__ import annotations
 
 import argparse
 import hashlib
 import json
+import os
 import re
 import shutil
 import subprocess
@@ -41,6 +52,9 @@ sys.path.insert(0, str(ROOT))
 from oracle import oracle as O  # noqa: E402
 
 BETA_DIR = "beta6_000000"
+# The reference checkout this script reads (override with --reference or LGF_REFERENCE).
+REFERENCE_LGF = os.environ.get("LGF_REFERENCE", "/root/reference/LGF")
+N_SAMPLE_SITES = 32
 
 
 def shape_dir(shape):
@@ -153,14 +167,55 @@ def write_flow_json(path, shape, steps, eps, meas, input_name, E, Q, csv_e, csv_
     path.write_text(json.dumps(rec, indent=1))
 
 
+def sample_sites(V, n=N_SAMPLE_SITES):
+    """n sites spread over the lattice (first, last and a prime stride between)."""
+    return sorted({0, V - 1, *[(k * 7919 * 97) % V for k in range(1, n - 1)]})[:n]
+
+
+def write_long_flow_json(path, shape, steps, eps, meas, input_name, E, Q, csv_e, csv_q, fname, flowed):
+    """Like write_flow_json, plus the flowed links of a spread of sites (the
+    first 72 doubles alone would only cover site 0)."""
+    write_flow_json(path, shape, steps, eps, meas, input_name, E, Q, csv_e, csv_q, fname, flowed)
+    rec = json.loads(path.read_text())
+    V = O.volume(shape)
+    sites = sample_sites(V)
+    rec["sample_sites"] = sites
+    rec["flowed_sites"] = flowed.reshape(V, 4 * 18)[sites].tolist()
+    path.write_text(json.dumps(rec, indent=1))
+
+
+def make_long(tmp: Path, which: str):
+    """The throughput configurations at their configured lengths and sizes."""
+    if which == "t3":
+        shape = (16, 16, 16, 16)
+        g = O.generate_G(shape, 7, 0.5)
+        res = reference_flow(tmp / "f16t3", g, shape, 300, 0.01, 10)
+        write_long_flow_json(HERE / "flow16_g7_t3.json", shape, 300, 0.01, 10,
+                             "generator G seed 7 scale 0.5", *res)
+    elif which == "bench":
+        shape = (48, 24, 24, 24)
+        g = O.generate_G(shape, 7, 0.5)
+        res = reference_flow(tmp / "f2448", g, shape, 3, 0.01, 3)
+        write_long_flow_json(HERE / "flow24x48_g7.json", shape, 3, 0.01, 3,
+                             "generator G seed 7 scale 0.5", *res)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=REFERENCE_LGF, help="the reference's LGF/ source directory")
     ap.add_argument("--skip-heatbath", action="store_true")
     ap.add_argument("--skip-16", action="store_true")
+    ap.add_argument("--only", choices=("small", "t3", "bench"), default=None,
+                    help="make only the small fixtures, or only one of the long flows")
     args = ap.parse_args()
-    O.build()
+    O.build(args.reference)
     if not O.reference_available():
         sys.exit("reference harness not built: the reference tree is needed to make fixtures")
+    if args.only in ("t3", "bench"):
+        with tempfile.TemporaryDirectory() as tmp:
+            make_long(Path(tmp), args.only)
+        print("golden fixtures written to", HERE)
+        return
     with tempfile.TemporaryDirectory() as tmp:
         tmp = Path(tmp)
         # ---- config 1: heatbath input + 8^4 flow
@@ -218,6 +273,9 @@ def main():
             g16 = O.generate_G(shape, 7, 0.5)
             res = reference_flow(tmp / "f16", g16, shape, 10, 0.01, 5)
             write_flow_json(HERE / "flow16_g7.json", shape, 10, 0.01, 5, "generator G seed 7 scale 0.5", *res)
+        if args.only is None:
+            make_long(tmp, "bench")
+            make_long(tmp, "t3")
     print("golden fixtures written to", HERE)
 
 

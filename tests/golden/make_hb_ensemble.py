@@ -10,6 +10,7 @@ hb8_ensemble.json beside this script.
     python tests/golden/make_hb_ensemble.py
 """
 import json
+import os
 import sys
 import tempfile
 from concurrent.futures import ThreadPoolExecutor
@@ -22,6 +23,8 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 from oracle import oracle as O  # noqa: E402
 
+# The reference checkout this script reads (override with LGF_REFERENCE).
+REFERENCE_LGF = os.environ.get("LGF_REFERENCE", "/root/reference/LGF")
 SHAPE = (8, 8, 8, 8)
 SEEDS = list(range(1, 10))
 
@@ -52,7 +55,7 @@ def one(seed, tmp):
 
 
 def main():
-    O.build()
+    O.build(REFERENCE_LGF)
     if not O.reference_available():
         sys.exit("reference harness not built: the reference tree is needed")
     with tempfile.TemporaryDirectory() as tmp, ThreadPoolExecutor(max_workers=len(SEEDS)) as ex:

@@ -24,7 +24,8 @@ def _run(args, timeout):
 
 @pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref/lgf_ref not built")
 def test_reference_arm_line():
-    d = _run(["--impl", "reference", "--steps", "1", "--warmup", "1", "--ref-procs", "2"], 600)
+    d = _run(["--impl", "reference", "--steps", "1", "--warmup", "1", "--ref-procs", "2", "--ref-shape", "8,8,8,8"],
+             600)
     assert d["impl"] == "reference" and d["metric"] == "site-RK3-steps/s" and d["unit"] == "site-RK3-steps/s"
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] == 2
@@ -43,8 +44,11 @@ def test_engine_arm_line():
     e = d["e2e"]
     assert e["value"] > 0 and e["h2d_bytes_per_step"] == 48 * 24 ** 3 * 576 and e["d2h_bytes_per_step"] > 0
     r = d["roofline"]
-    assert r["bound"] in ("hbm", "tensor") and r["unit"] == "GB/s"
+    # the stage kernel is bound by the FP64 FMA pipe; its HBM figures sit beside
+    assert r["bound"] == "fp64" and r["unit"] == "TFLOP/s"
     assert r["achieved"] > 0 and r["peak"] > 0 and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-9
+    h = r["hbm"]
+    assert h["unit"] == "GB/s" and h["achieved"] > 0 and abs(h["frac"] - h["achieved"] / h["peak"]) < 1e-9
     assert r["traffic"] is None or r["traffic"] > 0
     assert d["gpu_launches"] == 3 * 300 + 3 * 31
     assert set(d["clocks"]) >= {"sm_mhz", "sm_max_mhz", "reasons"}
