@@ -363,7 +363,8 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
         tmax = float(rng.uniform(1.0, 8.0))
         jobs.append(Job(shape, FP32MIXED, seed=1000 + i, nsteps=int(round(tmax / 0.01)), meas_every=5,
                         reunit_every=10))
-    gaps = rng.exponential(1.0 / rate, size=njobs)
+    # rate = inf: every job arrives at t = 0 (the saturated server)
+    gaps = np.zeros(njobs) if not np.isfinite(rate) else rng.exponential(1.0 / rate, size=njobs)
     try:
         import torch
         free, _ = torch.cuda.mem_get_info()
@@ -375,13 +376,14 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
         ids = []
         t0 = time.perf_counter()
         for j, g in zip(jobs, gaps):
-            time.sleep(float(g))
+            if g > 0:
+                time.sleep(float(g))
             ids.append(srv.submit(j))
         sts = [srv.wait(i, 3600.0) for i in ids]
         makespan = time.perf_counter() - t0
     lat = np.array([s.end_s - s.submit_s for s in sts])
     work = sum(int(np.prod(j.shape)) * j.nsteps for j in jobs)
-    return {"jobs": njobs, "rate_per_s": rate, "jobs_per_s": njobs / makespan,
+    return {"jobs": njobs, "rate_per_s": rate if np.isfinite(rate) else "all at t=0", "jobs_per_s": njobs / makespan,
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "site_steps_per_s": work / makespan, "hbm_budget_bytes": budget,
             "all_done": all(s.state == 2 for s in sts)}
@@ -501,6 +503,11 @@ def engine_arm(args):
                   "heatbath": lambda: form_heatbath(ctx)}
         wanted = list(makers) if args.forms == "all" else args.forms.split(",")
         forms = {k: makers[k]() for k in wanted}
+        if "served" in forms and "batched" in forms:
+            sat = [f for f in forms["served"] if f["rate_per_s"] == "all at t=0"]
+            if sat:
+                forms["served_saturated_vs_batched_fp32mixed"] = (
+                    sat[0]["site_steps_per_s"] / forms["batched"]["fp32mixed"]["site_steps_per_s"])
 
     launches_per_job = 3 * NSTEPS + 3 * nmeas + (NSTEPS // 10 if reunit else 0)
     line = {
@@ -574,8 +581,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the forms (volumes, FP32-mixed, batched, served, heatbath)")
     ap.add_argument("--forms", default="all", help="comma list of forms to run (default all)")
-    ap.add_argument("--serve-jobs", type=int, default=10, help="jobs per arrival rate of the served form")
-    ap.add_argument("--serve-rates", default="0.25,1.0", help="Poisson arrival rates (jobs/s) swept by the served form")
+    ap.add_argument("--serve-jobs", type=int, default=30, help="jobs per arrival rate of the served form")
+    ap.add_argument("--serve-rates", default="0.5,1.0,inf",
+                    help="Poisson arrival rates (jobs/s) swept by the served form; inf = all jobs at t = 0")
     ap.add_argument("--profile", action="store_true", help="one launch of each kernel (for ncu captures)")
     ap.add_argument("--profile-reps", type=int, default=1)
     args = ap.parse_args()

@@ -200,10 +200,27 @@ typedef struct lgf_batch_stats {
  * Results are identical to flowing each job alone with lgf_flow.  stats may be NULL. */
 int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats);
 
-/* Autotuner: time the candidate block shapes of the RK3 stage kernel for one
- * precision on a synthetic lattice and remember the fastest for this context
- * (also used by lgf_batch_run).  best_threads may be NULL. */
+/* Launch shapes and work orders of the RK3 stage and measurement kernels
+ * (no reference counterpart: the reference has no launch configuration).
+ * Every choice gives bit-identical results; only speed differs. */
+typedef struct lgf_tile_shape {
+    int stage_threads;    /* RK3 stage block size: 128, 256 or 384 (4 link directions x threads/4 sites) */
+    int stage_order;      /* 0: blocks of x1 rows swept through x0; 1: x1 columns walked per block */
+    int stage_budget_kb;  /* order 0: stage working set per row block and x0 slice */
+    int meas_budget_kb;   /* measurement: link bytes per row block and x0 slice (7 slices live) */
+    int meas_split;       /* measurement warps per plane: 1 (6-warp blocks) or 2 (12-warp blocks) */
+} lgf_tile_shape;
+
+/* Autotuner: time the candidate tile shapes for one precision on a lattice
+ * of this shape (generated links) with CUDA events, one parameter at a time,
+ * and remember the fastest in this context for lattices of this volume class
+ * (within a factor of two); lgf_flow, lgf_batch_run and the server use it.
+ * lgf_autotune returns only the stage block size.  best may be NULL. */
+int lgf_autotune_tiles(lgf_ctx* ctx, int precision, const int shape[4], lgf_tile_shape* best);
 int lgf_autotune(lgf_ctx* ctx, int precision, const int shape[4], int* best_threads);
+/* Set / read the shape used for this precision and volume class. */
+int lgf_set_tiles(lgf_ctx* ctx, int precision, const int shape[4], const lgf_tile_shape* tiles);
+int lgf_get_tiles(lgf_ctx* ctx, int precision, const int shape[4], lgf_tile_shape* tiles);
 
 /* ---------------------------------------------------------------- serving */
 typedef struct lgf_server lgf_server;

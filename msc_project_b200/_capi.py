@@ -51,6 +51,11 @@ class lgf_batch_stats(ctypes.Structure):
                 ("block_threads", ctypes.c_int)]
 
 
+class lgf_tile_shape(ctypes.Structure):
+    _fields_ = [("stage_threads", ctypes.c_int), ("stage_order", ctypes.c_int), ("stage_budget_kb", ctypes.c_int),
+                ("meas_budget_kb", ctypes.c_int), ("meas_split", ctypes.c_int)]
+
+
 class lgf_serve_config(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int), ("steps_per_tick", ctypes.c_int)]
 
@@ -91,6 +96,9 @@ SIGNATURES = {
     "lgf_overrelax": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lgf_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_job), ctypes.c_int, ctypes.POINTER(lgf_batch_stats)]),
     "lgf_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip]),
+    "lgf_autotune_tiles": (ctypes.c_int, [_vp, ctypes.c_int, _ip, ctypes.POINTER(lgf_tile_shape)]),
+    "lgf_set_tiles": (ctypes.c_int, [_vp, ctypes.c_int, _ip, ctypes.POINTER(lgf_tile_shape)]),
+    "lgf_get_tiles": (ctypes.c_int, [_vp, ctypes.c_int, _ip, ctypes.POINTER(lgf_tile_shape)]),
     "lgf_serve_start": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_serve_config), ctypes.POINTER(_vp)]),
     "lgf_serve_submit": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_job), ctypes.POINTER(ctypes.c_uint64)]),
     "lgf_serve_poll": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(lgf_job_status)]),

@@ -32,7 +32,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *ARCH]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall"]
 
-CU_SOURCES = ["lgf_engine.cu", "lgf_batch.cu", "lgf_serve.cu", "lgf_noalloc.cu", "lgf_heatbath.cu"]
+CU_SOURCES = ["lgf_engine.cu", "lgf_batch.cu", "lgf_serve.cu", "lgf_tune.cu", "lgf_noalloc.cu", "lgf_heatbath.cu"]
 CPP_SOURCES = ["lgf_dropin.cpp"]
 
 

@@ -45,16 +45,16 @@ int validate_job(lgf_ctx* ctx, const lgf_job& j) {
     return LGF_OK;
 }
 
-int tune_threads(lgf_ctx* ctx, int prec, const int shape[4], int* best);
-
-// block size for a wave whose largest lattice has this shape: tuned once per
+// tile shape for a wave whose largest lattice has this shape: tuned once per
 // precision and volume class (a small lattice prefers more, smaller blocks)
-int threads_for(lgf_ctx* ctx, int prec, const int shape[4]) {
+TileShape shape_for(lgf_ctx* ctx, int prec, const int shape[4]) {
     const long long V = 1LL * shape[0] * shape[1] * shape[2] * shape[3];
-    for (const auto& t : ctx->tuned)
-        if (t.prec == prec && V <= 2 * t.volume && t.volume <= 2 * V) return t.threads;
-    int best = default_threads(prec);
-    if (tune_threads(ctx, prec, shape, &best) == LGF_OK) record_tuned(ctx, prec, V, best);
+    if (has_tuned(ctx, prec, V)) return tuned_shape(ctx, prec, V);
+    TileShape best = default_shape(prec);
+    if (tune_shape(ctx, prec, shape, &best) != LGF_OK) {
+        ctx->err.clear();
+        return default_shape(prec);
+    }
     return best;
 }
 
@@ -83,10 +83,10 @@ int fetch_results(lgf_ctx* ctx, JobRun& r) {
 }
 
 // Flow one group of jobs (same precision) in lockstep; returns kernel launches.
-int run_group(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, int threads, int* launches) {
+int run_group(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, const TileShape& shape, int* launches) {
     long long tiles = 0;
-    for (auto* r : runs) tiles += (4LL * r->buf.g.V + threads - 1) / threads;
-    std::unique_ptr<GroupBase> grp(make_group(ctx, prec, threads, (int)runs.size(), std::max(tiles, 1LL), true));
+    for (auto* r : runs) tiles += (4LL * r->buf.g.V + shape.threads - 1) / shape.threads;
+    std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shape, (int)runs.size(), std::max(tiles, 1LL), true));
     if (!grp) return ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
     std::vector<LatticeBuf*> members;
     std::vector<double> eps;
@@ -186,67 +186,9 @@ std::vector<std::vector<JobRun*>> l2_waves(const std::vector<JobRun*>& jobs, int
     return waves;
 }
 
-int tune_threads(lgf_ctx* ctx, int prec, const int shape_in[4], int* best) {
-    // a lattice of the job's shape, capped so tuning stays well under a second
-    int shape[4] = {shape_in[0], shape_in[1], shape_in[2], shape_in[3]};
-    while (1LL * shape[0] * shape[1] * shape[2] * shape[3] > (1LL << 20) && shape[0] > 4) shape[0] = std::max(4, (shape[0] / 2) & ~1);
-    LatticeBuf b;
-    int rc = buf_alloc(ctx, b, shape, prec, 1);
-    if (rc != LGF_OK) return rc;
-    rc = launch_generate(ctx, b, 12345, 0.5);
-    b.eps = 0.01;
-    const int cands[] = {128, 256};  // multiples of 128: a tile holds all four directions of 32-site groups
-    float best_ms = 1e30f;
-    int best_t = default_threads(prec);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    for (int th : cands) {
-        if (rc != LGF_OK) break;
-        const long long tiles = (4LL * b.g.V + th - 1) / th;
-        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, th, 1, tiles, false));
-        if (!grp) continue;
-        std::vector<LatticeBuf*> m{&b};
-        if (grp->set_members(m) != LGF_OK) continue;
-        grp->launch_step();  // warm-up
-        cudaEventRecord(e0, ctx->stream);
-        for (int i = 0; i < 3; ++i) grp->launch_step();
-        cudaEventRecord(e1, ctx->stream);
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = set_error(ctx, LGF_ECUDA, "autotune timing failed");
-            break;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best_t = th;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaStreamSynchronize(ctx->stream);
-    buf_free(b);
-    if (rc == LGF_OK) *best = best_t;
-    return rc;
-}
-
 }  // namespace
 
 extern "C" {
-
-int lgf_autotune(lgf_ctx* ctx, int precision, const int shape[4], int* best_threads) {
-    if (!ctx) return LGF_EINVAL;
-    if (precision != LGF_PREC_FP64 && precision != LGF_PREC_FP32MIXED) return LGF_EINVAL;
-    if (!valid_shape(shape)) return set_error(ctx, LGF_EINVAL, "autotune shape must be even and >= 4");
-    cudaSetDevice(ctx->device);
-    int best = 0;
-    int rc = tune_threads(ctx, precision, shape, &best);
-    if (rc != LGF_OK) return rc;
-    record_tuned(ctx, precision, 1LL * shape[0] * shape[1] * shape[2] * shape[3], best);
-    if (best_threads) *best_threads = best;
-    return LGF_OK;
-}
 
 int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats) {
     if (!ctx || (!jobs && njobs > 0) || njobs < 0) return LGF_EINVAL;
@@ -279,7 +221,7 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
     // group the jobs by precision and pick each group's block size (autotuned
     // once per context, before the timed region)
     std::vector<JobRun*> groups[2];
-    int threads[2] = {0, 0};
+    TileShape shapes[2];
     for (int prec = 0; prec < 2; ++prec) {
         int big[4] = {4, 4, 4, 4};
         long long bigV = 0;
@@ -291,7 +233,7 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
                     std::memcpy(big, r->job->shape, sizeof big);
                 }
             }
-        if (!groups[prec].empty()) threads[prec] = threads_for(ctx, prec, big);
+        if (!groups[prec].empty()) shapes[prec] = shape_for(ctx, prec, big);
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -300,9 +242,9 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
     cudaEventRecord(e0, ctx->stream);
     for (int prec = 0; prec < 2 && rc == LGF_OK; ++prec) {
         if (groups[prec].empty()) continue;
-        threads_used = threads[prec];
+        threads_used = shapes[prec].threads;
         for (auto& wave : l2_waves(groups[prec], prec)) {
-            rc = run_group(ctx, prec, wave, threads[prec], &launches);
+            rc = run_group(ctx, prec, wave, shapes[prec], &launches);
             if (rc != LGF_OK) break;
         }
     }

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "lgf_engine.cuh"
+#include "lgf_tiles.h"
 
 namespace lgf {
 
@@ -56,29 +57,49 @@ size_t footprint_bytes(const int shape[4], int precision, int meas_slots) {
 // directions: one block per SM whose eight warps share their neighbours in
 // L1; 9% faster per stage than 128 on 24^3x48, 19% per job on 48^4), FP32 128
 // (three blocks per SM; 256 is 20% slower).
-int default_threads(int precision) { return precision == LGF_PREC_FP64 ? 256 : 128; }
+#ifndef LGF_FP64_THREADS
+#define LGF_FP64_THREADS 256
+#endif
+#ifndef LGF_FP32_THREADS
+#define LGF_FP32_THREADS 128
+#endif
+int default_threads(int precision) { return precision == LGF_PREC_FP64 ? LGF_FP64_THREADS : LGF_FP32_THREADS; }
+
+TileShape default_shape(int precision) {
+    TileShape t;
+    t.threads = default_threads(precision);
+    return t;
+}
 
 static const lgf_ctx::Tuned* find_tuned(const lgf_ctx* ctx, int precision, long long volume) {
+    const lgf_ctx::Tuned* best = nullptr;
     for (const auto& t : ctx->tuned)
-        if (t.prec == precision && volume <= 2 * t.volume && t.volume <= 2 * volume) return &t;
-    return nullptr;
+        if (t.prec == precision && volume <= 2 * t.volume && t.volume <= 2 * volume)
+            if (!best || std::llabs(t.volume - volume) < std::llabs(best->volume - volume)) best = &t;
+    return best;
 }
 
-int stage_threads(const lgf_ctx* ctx, int precision, long long volume) {
+TileShape tuned_shape(const lgf_ctx* ctx, int precision, long long volume) {
     const lgf_ctx::Tuned* t = find_tuned(ctx, precision, volume);
-    return t ? t->threads : default_threads(precision);
+    return t ? t->shape : default_shape(precision);
 }
 
-void record_tuned(lgf_ctx* ctx, int precision, long long volume, int threads) {
+bool has_tuned(const lgf_ctx* ctx, int precision, long long volume) { return find_tuned(ctx, precision, volume) != nullptr; }
+
+void record_tuned(lgf_ctx* ctx, int precision, long long volume, const TileShape& shape) {
     for (auto& t : ctx->tuned)
         if (t.prec == precision && t.volume == volume) {
-            t.threads = threads;
+            t.shape = shape;
             return;
         }
-    ctx->tuned.push_back({precision, volume, threads});
+    ctx->tuned.push_back({precision, volume, shape});
 }
 
 void buf_free(LatticeBuf& b) {
+    if (b.placed) {  // the memory belongs to the caller (a server's arena)
+        b = LatticeBuf();
+        return;
+    }
     if (b.U[0]) cudaFree(b.U[0]);  // U[1], U[2] lie in the same allocation
     if (b.A) cudaFree(b.A);
     if (b.partial) cudaFree(b.partial);
@@ -122,8 +143,47 @@ int buf_alloc(lgf_ctx* ctx, LatticeBuf& b, const int shape[4], int precision, in
     return LGF_OK;
 }
 
+// The same buffers laid out inside one block of caller memory, each part
+// starting on a 256-byte boundary (placed_bytes gives the block's size).
+static inline size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+size_t placed_bytes(const int shape[4], int precision, int meas_slots) {
+    const size_t V = (size_t)shape[0] * shape[1] * shape[2] * shape[3], Vp = padded_sites(V);
+    const size_t rs = real_size(precision);
+    const size_t nchunk = ((size_t)shape[1] * shape[2] * shape[3] + MEAS_SITES - 1) / MEAS_SITES;
+    return align256(3 * Vp * 4 * 18 * rs) + align256(Vp * 4 * 8 * rs) +
+           align256((size_t)shape[0] * nchunk * sizeof(double2)) + align256((size_t)shape[0] * sizeof(double2)) +
+           align256(sizeof(int)) + align256((size_t)std::max(meas_slots, 1) * (2 + 2 * (size_t)shape[0]) * sizeof(double));
+}
+
+void buf_place(LatticeBuf& b, const int shape[4], int precision, int meas_slots, void* mem) {
+    b = LatticeBuf();
+    b.g = make_geom(shape);
+    b.prec = precision;
+    b.placed = true;
+    const size_t Vp = padded_sites((size_t)b.g.V), rs = real_size(precision);
+    b.nchunk = (b.g.Vs + MEAS_SITES - 1) / MEAS_SITES;
+    char* p = (char*)mem;
+    const size_t ring = Vp * 4 * 18 * rs;
+    b.U[0] = p;
+    b.U[1] = p + ring;
+    b.U[2] = p + 2 * ring;
+    p += align256(3 * ring);
+    b.A = p;
+    p += align256(Vp * 4 * 8 * rs);
+    b.partial = (double2*)p;
+    p += align256((size_t)b.g.n[0] * b.nchunk * sizeof(double2));
+    b.slice_sums = (double2*)p;
+    p += align256((size_t)b.g.n[0] * sizeof(double2));
+    b.slot = (int*)p;
+    p += align256(sizeof(int));
+    b.meas_cap = std::max(meas_slots, 1);
+    b.meas = (double*)p;
+}
+
 int buf_grow_meas(lgf_ctx* ctx, LatticeBuf& b, int meas_slots) {
     if (meas_slots <= b.meas_cap) return LGF_OK;
+    if (b.placed) return set_error(ctx, LGF_EINVAL, "a placed lattice holds %d measurement slots", b.meas_cap);
     double* m = nullptr;
     cudaError_t e = cudaMalloc(&m, (size_t)meas_slots * (2 + 2 * (size_t)b.g.n[0]) * sizeof(double));
     if (e != cudaSuccess) {
@@ -142,131 +202,122 @@ int count_measurements(const lgf_flow_opts& o) {
     return n;
 }
 
-// ------------------------------------------------------------ work order
-// The persistent kernels take tiles in list order, so the list order sets the
-// L2 reuse distance of the stencil.  In plain site order the x0 +- 1 (and, in
-// the measurement, up to +- 3) neighbours of a site are reused one slice of
-// work later; once a slice of work exceeds the L2 budget they come from HBM
-// again.  Large lattices are therefore ordered in blocks of x1 (and x2) rows,
-// each block swept through every x0 slice before the next block starts.  Only
-// the order changes: the set of tiles is the same, and no result depends on
-// it (no reduction runs in tile order).
-// Block budgets, measured on 16^4 .. 48^4 (FP64, 100 steps): 8 MB / 2 MB gave
-// +5% on 24^3x48 and +7% on 32^4 over the plain site order; 24/8, 12/4, 4/1
-// and smaller were between the two.
-#ifndef LGF_STAGE_L2_MB
-#define LGF_STAGE_L2_MB 8  // MB of stage work per block and slice
-#endif
-#ifndef LGF_MEAS_L2_MB
-#define LGF_MEAS_L2_MB 2  // MB of links read per block and slice (x0 +- 3: 7 slices live)
-#endif
-static const double STAGE_L2_BUDGET = LGF_STAGE_L2_MB * double(1 << 20);
-static const double MEAS_L2_BUDGET = LGF_MEAS_L2_MB * double(1 << 20);
-
-// A block: x1 in [a1, b1), x2 in [a2, b2), all x3.  One block per slice when
-// a slice of work fits the budget; else blocks of whole x1 rows, at least
-// MIN_ROWS deep so that most x1 neighbours stay inside; else (lattices whose
-// x1 rows are themselves large) square (x1, x2) blocks.
-struct SiteBlock { int a1, b1, a2, b2; };
-#ifndef LGF_MIN_ROWS
-#define LGF_MIN_ROWS 4
-#endif
-static const int MIN_ROWS = LGF_MIN_ROWS;
-
-static std::vector<SiteBlock> site_blocks(const Geom& g, double budget, double bytes_per_site) {
-    std::vector<SiteBlock> out;
-    const int N1 = g.n[1], N2 = g.n[2], N3 = g.n[3];
-    const double sites = budget / bytes_per_site;  // sites of one block and slice
-    if ((double)g.Vs <= sites) {
-        out.push_back({0, N1, 0, N2});
-    } else if ((double)MIN_ROWS * N2 * N3 <= sites) {
-        const int r = std::max(1, (int)(sites / ((double)N2 * N3)));
-        for (int a = 0; a < N1; a += r) out.push_back({a, std::min(a + r, N1), 0, N2});
-    } else {
-        const int side = std::max(1, (int)std::sqrt(sites / N3));
-        for (int a = 0; a < N1; a += side)
-            for (int c = 0; c < N2; c += side) out.push_back({a, std::min(a + side, N1), c, std::min(c + side, N2)});
+// The measurement lists of a subset of a group's members, assembled on the
+// device from the per-member segments of the group's full measurement tile
+// list (built once per change of members), so that choosing which members a
+// measurement covers is one small copy and this launch, with no host wait.
+//   sel = [nsel, total tiles, total slices,
+//          then per selected member k: member, segment offset, tiles, first
+//          output tile, N0, first output slice]
+// Outputs: mtiles (the selected segments back to back), rtiles (member, t)
+// for t < N0, jobs[k] = member, counts = {tiles, slices, nsel}.  Grid
+// (max(nsel, 1), any): block (k, y) copies a share of segment k.
+constexpr int SEL_HEADER = 3, SEL_FIELDS = 6;
+__global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ sel, const int4* __restrict__ all,
+                                                        int4* __restrict__ mtiles, int2* __restrict__ rtiles,
+                                                        int* __restrict__ jobs, int* __restrict__ counts) {
+    const int nsel = sel[0];
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        counts[0] = sel[1];
+        counts[1] = sel[2];
+        counts[2] = nsel;
     }
-    return out;
-}
-
-// stage tiles of T consecutive sites (first site a multiple of T) of lattice
-// i, each assigned to the block row that holds its first site
-static void append_stage_tiles(std::vector<int2>& tiles, int i, const Geom& g, int T, double bytes_per_site) {
-    const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
-    for (const SiteBlock& b : site_blocks(g, STAGE_L2_BUDGET, bytes_per_site))
-        for (long long x0 = 0; x0 < g.n[0]; ++x0)
-            for (long long x1 = b.a1; x1 < b.b1; ++x1) {
-                const long long base = x0 * g.Vs + x1 * row;
-                const long long lo = base + b.a2 * N3, hi = base + b.b2 * N3;
-                for (long long s0 = (lo + T - 1) / T * T; s0 < hi; s0 += T) tiles.push_back(make_int2(i, (int)s0));
-            }
-}
-
-#ifndef LGF_STAGE_ORDER
-#define LGF_STAGE_ORDER 1  // stage tile order: 0 blocks of x1 rows swept through x0, 1 x1 columns per CTA
-#endif
-// Column order: a column is the tiles at one (x0, position in the x1 row) for
-// x1 = 0..N1-1.  Columns are taken G at a time (G = the persistent grid) and
-// listed row by row, so CTA b walks column b along x1: the x1 - 1 neighbours
-// of its tile are the links of the tile it did before.  Needs tiles that lie
-// inside one x1 row (N2 N3 a multiple of T) and bands of G columns that span
-// at least 8 x0 slices (else most x0 neighbours fall on a band edge: 48^4
-// with 64-site tiles spans 4); returns false otherwise.  Measured against the
-// blocked order: +3-4% flow-only on 24^3x48 and 32^4.
-static bool append_stage_tiles_columns(std::vector<int2>& tiles, int i, const Geom& g, int T, int G) {
-    const long long row = (long long)g.n[2] * g.n[3];
-    if (row % T || G < 1) return false;
-    const long long per_row = row / T, ncol = g.n[0] * per_row;
-    if (8 * per_row > G && ncol > G) return false;
-    for (long long c0 = 0; c0 < ncol; c0 += G) {
-        const long long c1 = std::min(c0 + (long long)G, ncol);
-        for (long long x1 = 0; x1 < g.n[1]; ++x1)
-            for (long long c = c0; c < c1; ++c)
-                tiles.push_back(make_int2(i, (int)((c / per_row) * g.Vs + x1 * row + (c % per_row) * T)));
+    const int k = blockIdx.x;
+    if (k >= nsel) return;
+    const int* f = sel + SEL_HEADER + SEL_FIELDS * k;
+    const int member = f[0], off = f[1], n = f[2], mstart = f[3], n0 = f[4], rstart = f[5];
+    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += gridDim.y * blockDim.x)
+        mtiles[mstart + i] = all[off + i];
+    if (blockIdx.y == 0) {
+        for (int t = threadIdx.x; t < n0; t += blockDim.x) rtiles[rstart + t] = make_int2(member, t);
+        if (threadIdx.x == 0) jobs[k] = member;
     }
-    return true;
 }
 
-// measurement tiles (lattice, slice, 32-site chunk of the slice) of lattice i
-static void append_measure_tiles(std::vector<int4>& tiles, int i, const Geom& g, double bytes_per_site) {
-    const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
-    for (const SiteBlock& b : site_blocks(g, MEAS_L2_BUDGET, bytes_per_site))
-        for (int t = 0; t < g.n[0]; ++t)
-            for (long long x1 = b.a1; x1 < b.b1; ++x1) {
-                const long long lo = x1 * row + b.a2 * N3, hi = x1 * row + b.b2 * N3;
-                for (long long c = (lo + MEAS_SITES - 1) / MEAS_SITES; c * MEAS_SITES < hi; ++c)
-                    tiles.push_back(make_int4(i, t, (int)c, 0));
-            }
-}
+// ---------------------------------------------------------- pinned staging
+// Page-locked areas for the host->device copies of a group's lists.  A copy
+// from pageable memory may make the driver wait for the stream; from these
+// areas it never does.  Two areas are used in turn, and one is rewritten only
+// after the copies that last read it have completed (its event) -- normally
+// long before, since the other area was used in between.
+class PinnedStage {
+public:
+    ~PinnedStage() {
+        for (int k = 0; k < 2; ++k) {
+            if (ev_[k]) cudaEventSynchronize(ev_[k]);
+            if (ev_[k]) cudaEventDestroy(ev_[k]);
+            if (buf_[k]) cudaFreeHost(buf_[k]);
+        }
+    }
+    // an area of at least n bytes for the next copies
+    cudaError_t acquire(size_t n, char** out) {
+        cur_ ^= 1;
+        cudaError_t e = cudaSuccess;
+        if (!ev_[cur_]) e = cudaEventCreateWithFlags(&ev_[cur_], cudaEventDisableTiming);
+        else e = cudaEventSynchronize(ev_[cur_]);
+        if (e != cudaSuccess) return e;
+        if (cap_[cur_] < n) {
+            if (buf_[cur_]) cudaFreeHost(buf_[cur_]);
+            buf_[cur_] = nullptr;
+            cap_[cur_] = 0;
+            const size_t c = std::max<size_t>(n + n / 2, 4096);
+            e = cudaMallocHost(&buf_[cur_], c);
+            if (e != cudaSuccess) return e;
+            cap_[cur_] = c;
+        }
+        *out = buf_[cur_];
+        return cudaSuccess;
+    }
+    // the copies from the current area have been issued on stream s
+    cudaError_t release(cudaStream_t s) { return cudaEventRecord(ev_[cur_], s); }
+
+private:
+    char* buf_[2] = {nullptr, nullptr};
+    size_t cap_[2] = {0, 0};
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    int cur_ = 1;
+};
+
+static inline size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
 
 // ------------------------------------------------------------------ groups
 template <typename R> class Group : public GroupBase {
 public:
-    Group(lgf_ctx* ctx, int threads, int max_members, long long max_tiles, bool dynamic)
-        : ctx_(ctx), threads_(threads), max_members_(max_members), max_tiles_(max_tiles), dynamic_(dynamic) {}
+    Group(lgf_ctx* ctx, const TileShape& shape, int max_members, long long max_tiles, bool dynamic)
+        : ctx_(ctx), shape_(shape), threads_(shape.threads), max_members_(max_members), max_tiles_(max_tiles),
+          dynamic_(dynamic) {}
     ~Group() override {
+        cudaStreamSynchronize(ctx_->stream);  // the lists and the staging areas are in use until then
         if (step_exec_) cudaGraphExecDestroy(step_exec_);
         if (meas_exec_) cudaGraphExecDestroy(meas_exec_);
         cudaFree(d_desc_);
         cudaFree(d_tiles_);
         cudaFree(d_mtiles_);
+        cudaFree(d_all_mtiles_);
         cudaFree(d_rtiles_);
         cudaFree(d_jobs_);
         cudaFree(d_counts_);
+        cudaFree(d_sel_);
     }
 
     int init() {
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_desc_, sizeof(LatDesc<R>) * max_members_));
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_tiles_, sizeof(int2) * max_tiles_));
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_counts_, sizeof(int) * 4));
+        LGF_CUDA_TRY(ctx_, cudaMalloc(&d_sel_, sizeof(int) * (SEL_HEADER + SEL_FIELDS * (size_t)max_members_)));
         LGF_CUDA_TRY(ctx_, cudaMemsetAsync(d_counts_, 0, sizeof(int) * 4, ctx_->stream));
         int nb = 0;
         LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rk3_stage<R, 1>, threads_, 0));
         stage_grid_max_ = std::max(1, nb) * ctx_->sm_count;
-        LGF_CUDA_TRY(ctx_, prepare_measure_kernel<R>());
-        LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R>, MEAS_SITES * MEAS_WARPS,
-                                                                         measure_smem_bytes<R>()));
+        if (shape_.meas_split == 2) {
+            LGF_CUDA_TRY(ctx_, (prepare_measure_kernel<R, false, 2>()));
+            LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R, false, 2>,
+                                                                             MEAS_SITES * 12, measure_smem_bytes<R>()));
+        } else {
+            LGF_CUDA_TRY(ctx_, (prepare_measure_kernel<R, false, 1>()));
+            LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_measure<R, false, 1>,
+                                                                             MEAS_SITES * 6, measure_smem_bytes<R>()));
+        }
         meas_grid_max_ = std::max(1, nb) * ctx_->sm_count;
         if (dynamic_) {
             // members change after capture: size the measurement lists for the
@@ -275,6 +326,7 @@ public:
             rtiles_cap_ = 256LL * max_members_;
             jobs_cap_ = max_members_;
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_mtiles_, sizeof(int4) * mtiles_cap_));
+            LGF_CUDA_TRY(ctx_, cudaMalloc(&d_all_mtiles_, sizeof(int4) * mtiles_cap_));
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_rtiles_, sizeof(int2) * rtiles_cap_));
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_jobs_, sizeof(int) * jobs_cap_));
         }
@@ -287,7 +339,9 @@ public:
         members_ = members;
         h_desc_.resize(members.size());
         std::vector<int2> tiles;
-        long long mt = 0;
+        std::vector<int4> mtiles;
+        seg_off_.assign(members.size(), 0);
+        seg_len_.assign(members.size(), 0);
         for (size_t i = 0; i < members.size(); ++i) {
             const LatticeBuf& b = *members[i];
             LatDesc<R>& d = h_desc_[i];
@@ -304,34 +358,32 @@ public:
             d.eps = (R)b.eps;
             // a tile is threads_/4 consecutive sites with all four link directions;
             // per site a stage reads and writes 4 links and 4 su(3) accumulators
-            if (!(LGF_STAGE_ORDER == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
-                append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, 4.0 * (2 * 18 + 8) * sizeof(R));
-            mt += (long long)b.g.n[0] * b.nchunk;
+            if (!(shape_.stage_order == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
+                append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, shape_.stage_budget, 4.0 * (2 * 18 + 8) * sizeof(R));
+            // this member's segment of the measurement list
+            seg_off_[i] = (int)mtiles.size();
+            append_measure_tiles(mtiles, (int)i, b.g, shape_.meas_budget, 4.0 * 18 * sizeof(R));
+            seg_len_[i] = (int)mtiles.size() - seg_off_[i];
         }
         if ((long long)tiles.size() > max_tiles_)
             return set_error(ctx_, LGF_EINVAL, "work list of %zu tiles exceeds the group capacity %lld", tiles.size(),
                              max_tiles_);
-        ntiles_ = (int)tiles.size();
-        if (!members.empty())
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h_desc_.data(), sizeof(LatDesc<R>) * members.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
-        if (ntiles_)
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_tiles_, tiles.data(), sizeof(int2) * tiles.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
-        h_counts_[0] = ntiles_;
-        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_counts_, &h_counts_[0], sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
-        // measurement lists sized for every member at once
+        const long long mt = (long long)mtiles.size();
         if (mt > mtiles_cap_) {
-            cudaFree(d_mtiles_);
-            d_mtiles_ = nullptr;
             if (step_exec_ || meas_exec_) return set_error(ctx_, LGF_EINVAL, "measurement list grew after capture");
+            LGF_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
+            cudaFree(d_mtiles_);
+            cudaFree(d_all_mtiles_);
+            d_mtiles_ = d_all_mtiles_ = nullptr;
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_mtiles_, sizeof(int4) * std::max(mt, 1LL)));
+            LGF_CUDA_TRY(ctx_, cudaMalloc(&d_all_mtiles_, sizeof(int4) * std::max(mt, 1LL)));
             mtiles_cap_ = mt;
         }
         long long rt = 0;
         for (auto* b : members) rt += b->g.n[0];
         if (rt > rtiles_cap_ || (long long)members.size() > jobs_cap_) {
             if (step_exec_ || meas_exec_) return set_error(ctx_, LGF_EINVAL, "reduction list grew after capture");
+            LGF_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
             cudaFree(d_rtiles_);
             cudaFree(d_jobs_);
             rtiles_cap_ = std::max(rt, (long long)max_members_ * 64);
@@ -339,45 +391,74 @@ public:
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_rtiles_, sizeof(int2) * rtiles_cap_));
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_jobs_, sizeof(int) * jobs_cap_));
         }
+        ntiles_ = (int)tiles.size();
+        // one page-locked area carries the descriptors, both tile lists and the count
+        const size_t bd = align16(sizeof(LatDesc<R>) * members.size()), bt = align16(sizeof(int2) * tiles.size()),
+                     bm = align16(sizeof(int4) * mtiles.size());
+        char* h = nullptr;
+        LGF_CUDA_TRY(ctx_, stage_.acquire(bd + bt + bm + 16, &h));
+        std::memcpy(h, h_desc_.data(), sizeof(LatDesc<R>) * members.size());
+        std::memcpy(h + bd, tiles.data(), sizeof(int2) * tiles.size());
+        std::memcpy(h + bd + bt, mtiles.data(), sizeof(int4) * mtiles.size());
+        std::memcpy(h + bd + bt + bm, &ntiles_, sizeof(int));
+        if (!members.empty())
+            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h, sizeof(LatDesc<R>) * members.size(), cudaMemcpyHostToDevice,
+                                               ctx_->stream));
+        if (ntiles_)
+            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_tiles_, h + bd, sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice,
+                                               ctx_->stream));
+        if (mt)
+            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_all_mtiles_, h + bd + bt, sizeof(int4) * mtiles.size(),
+                                               cudaMemcpyHostToDevice, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_counts_, h + bd + bt + bm, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
         return LGF_OK;
     }
 
     int set_eps(const std::vector<double>& eps) override {
         for (size_t i = 0; i < h_desc_.size() && i < eps.size(); ++i) h_desc_[i].eps = (R)eps[i];
-        if (!h_desc_.empty())
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h_desc_.data(), sizeof(LatDesc<R>) * h_desc_.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
+        if (h_desc_.empty()) return LGF_OK;
+        char* h = nullptr;
+        LGF_CUDA_TRY(ctx_, stage_.acquire(sizeof(LatDesc<R>) * h_desc_.size(), &h));
+        std::memcpy(h, h_desc_.data(), sizeof(LatDesc<R>) * h_desc_.size());
+        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h, sizeof(LatDesc<R>) * h_desc_.size(), cudaMemcpyHostToDevice,
+                                           ctx_->stream));
+        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
         return LGF_OK;
     }
 
+    // The selection table goes through a page-locked area and the lists are
+    // assembled on the device (k_select_measure): no host wait.
     int set_measured(const std::vector<int>& which) override {
-        h_mtiles_.clear();
-        h_rtiles_.clear();
-        h_jobs_.clear();
-        for (int i : which) {
-            const LatticeBuf& b = *members_[i];
-            append_measure_tiles(h_mtiles_, i, b.g, 4.0 * 18 * sizeof(R));
-            for (int t = 0; t < b.g.n[0]; ++t) h_rtiles_.push_back(make_int2(i, t));
-            h_jobs_.push_back(i);
+        if ((int)which.size() > max_members_) return set_error(ctx_, LGF_EINVAL, "measurement list exceeds capacity");
+        std::vector<int> sel(SEL_HEADER + SEL_FIELDS * which.size());
+        long long tm = 0, tr = 0;
+        for (size_t k = 0; k < which.size(); ++k) {
+            const int i = which[k];
+            if (i < 0 || i >= (int)members_.size()) return set_error(ctx_, LGF_EINVAL, "no member %d to measure", i);
+            int* f = &sel[SEL_HEADER + SEL_FIELDS * k];
+            f[0] = i;
+            f[1] = seg_off_[i];
+            f[2] = seg_len_[i];
+            f[3] = (int)tm;
+            f[4] = members_[i]->g.n[0];
+            f[5] = (int)tr;
+            tm += seg_len_[i];
+            tr += members_[i]->g.n[0];
         }
-        if ((long long)h_mtiles_.size() > mtiles_cap_ || (long long)h_rtiles_.size() > rtiles_cap_ ||
-            (long long)h_jobs_.size() > jobs_cap_)
+        if (tm > mtiles_cap_ || tr > rtiles_cap_ || (long long)which.size() > jobs_cap_)
             return set_error(ctx_, LGF_EINVAL, "measurement list exceeds capacity");
-        if (!h_mtiles_.empty()) {
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_mtiles_, h_mtiles_.data(), sizeof(int4) * h_mtiles_.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_rtiles_, h_rtiles_.data(), sizeof(int2) * h_rtiles_.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
-            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_jobs_, h_jobs_.data(), sizeof(int) * h_jobs_.size(),
-                                               cudaMemcpyHostToDevice, ctx_->stream));
-        }
-        h_counts_[1] = (int)h_mtiles_.size();
-        h_counts_[2] = (int)h_rtiles_.size();
-        h_counts_[3] = (int)h_jobs_.size();
-        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_counts_ + 1, &h_counts_[1], 3 * sizeof(int), cudaMemcpyHostToDevice,
-                                           ctx_->stream));
-        // the host copy must outlive the async copies: wait for them here
-        LGF_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
+        sel[0] = (int)which.size();
+        sel[1] = (int)tm;
+        sel[2] = (int)tr;
+        char* h = nullptr;
+        LGF_CUDA_TRY(ctx_, stage_.acquire(sizeof(int) * sel.size(), &h));
+        std::memcpy(h, sel.data(), sizeof(int) * sel.size());
+        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sel_, h, sizeof(int) * sel.size(), cudaMemcpyHostToDevice, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
+        k_select_measure<<<dim3(std::max<int>(1, (int)which.size()), 16), 256, 0, ctx_->stream>>>(
+            d_sel_, d_all_mtiles_, d_mtiles_, d_rtiles_, d_jobs_, d_counts_ + 1);
+        LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
     }
 
@@ -413,8 +494,7 @@ public:
             if (k == 1) k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
             if (k == 2) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
         } else {
-            k_measure<R><<<meas_grid(), dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R>(), ctx_->stream>>>(
-                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
+            launch_measure_kernel(meas_grid());
         }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
@@ -425,8 +505,7 @@ public:
         const int mg = meas_grid();
         const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
         const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
-        k_measure<R><<<mg, dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R>(), ctx_->stream>>>(
-            d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
+        launch_measure_kernel(mg);
         k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
         k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
@@ -466,8 +545,18 @@ public:
     }
     int launches_per_step() const override { return 3; }
     int threads() const override { return threads_; }
+    const TileShape& shape() const override { return shape_; }
 
 private:
+    void launch_measure_kernel(int grid) {
+        if (shape_.meas_split == 2)
+            k_measure<R, false, 2><<<grid, dim3(MEAS_SITES, 12), measure_smem_bytes<R>(), ctx_->stream>>>(
+                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
+        else
+            k_measure<R, false, 1><<<grid, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
+    }
+
     int capture_one(bool step, cudaGraphExec_t* out) {
         cudaGraph_t graph = nullptr;
         LGF_CUDA_TRY(ctx_, cudaStreamBeginCapture(ctx_->stream, cudaStreamCaptureModeThreadLocal));
@@ -485,19 +574,20 @@ private:
     }
 
     lgf_ctx* ctx_;
+    TileShape shape_;
     int threads_;
     int max_members_;
     long long max_tiles_;
     bool dynamic_;
     std::vector<LatticeBuf*> members_;
     std::vector<LatDesc<R>> h_desc_;
-    std::vector<int4> h_mtiles_;
-    std::vector<int2> h_rtiles_;
-    std::vector<int> h_jobs_;
-    int h_counts_[4] = {0, 0, 0, 0};
+    std::vector<int> seg_off_, seg_len_;  // each member's segment of d_all_mtiles_
+    PinnedStage stage_;
     LatDesc<R>* d_desc_ = nullptr;
     int2* d_tiles_ = nullptr;
-    int4* d_mtiles_ = nullptr;
+    int4* d_mtiles_ = nullptr;      // the measured members' tiles (k_select_measure)
+    int4* d_all_mtiles_ = nullptr;  // every member's measurement tiles
+    int* d_sel_ = nullptr;          // selection table of the next measurement
     int2* d_rtiles_ = nullptr;
     int* d_jobs_ = nullptr;
     int* d_counts_ = nullptr;  // ntiles, nmtiles, nrtiles, njobs
@@ -508,14 +598,21 @@ private:
     cudaGraphExec_t step_exec_ = nullptr, meas_exec_ = nullptr;
 };
 
-GroupBase* make_group(lgf_ctx* ctx, int precision, int threads, int max_members, long long max_tiles, bool dynamic) {
+GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
+                      bool dynamic) {
+    if (shape.threads < 128 || shape.threads % 128 || shape.threads > LGF_STAGE_MAXT ||
+        (shape.meas_split != 1 && shape.meas_split != 2) || shape.stage_budget <= 0 || shape.meas_budget <= 0) {
+        set_error(ctx, LGF_EINVAL, "invalid tile shape (threads %d, measurement split %d)", shape.threads,
+                  shape.meas_split);
+        return nullptr;
+    }
     GroupBase* g = nullptr;
     if (precision == LGF_PREC_FP64) {
-        auto* p = new (std::nothrow) Group<double>(ctx, threads, max_members, max_tiles, dynamic);
+        auto* p = new (std::nothrow) Group<double>(ctx, shape, max_members, max_tiles, dynamic);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     } else {
-        auto* p = new (std::nothrow) Group<float>(ctx, threads, max_members, max_tiles, dynamic);
+        auto* p = new (std::nothrow) Group<float>(ctx, shape, max_members, max_tiles, dynamic);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     }
@@ -526,15 +623,19 @@ GroupBase* make_group(lgf_ctx* ctx, int precision, int threads, int max_members,
 static inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 // one block per 32-site layout block (the transpose kernels above)
-int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file) {
+static int launch_to_device_on(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file, cudaStream_t st) {
     const int V = b.g.V;
     const int nb = blocks_for(V, LAYOUT_BLOCK);
     if (b.prec == LGF_PREC_FP64)
-        k_to_device<double><<<nb, CONV_THREADS, 0, ctx->stream>>>((const double2*)dev_file, (cplx<double>*)b.U[0], V);
+        k_to_device<double><<<nb, CONV_THREADS, 0, st>>>((const double2*)dev_file, (cplx<double>*)b.U[0], V);
     else
-        k_to_device<float><<<nb, CONV_THREADS, 0, ctx->stream>>>((const double2*)dev_file, (cplx<float>*)b.U[0], V);
+        k_to_device<float><<<nb, CONV_THREADS, 0, st>>>((const double2*)dev_file, (cplx<float>*)b.U[0], V);
     LGF_CUDA_TRY(ctx, cudaGetLastError());
     return LGF_OK;
+}
+
+int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file) {
+    return launch_to_device_on(ctx, b, dev_file, ctx->stream);
 }
 
 int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file) {
@@ -548,14 +649,18 @@ int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file) {
     return LGF_OK;
 }
 
-int launch_generate(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale) {
+int launch_generate_on(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale, cudaStream_t st) {
     const int V = b.g.V;
     if (b.prec == LGF_PREC_FP64)
-        k_generate_G<double><<<blocks_for(4LL * V, 128), 128, 0, ctx->stream>>>((cplx<double>*)b.U[0], V, seed, scale);
+        k_generate_G<double><<<blocks_for(4LL * V, 128), 128, 0, st>>>((cplx<double>*)b.U[0], V, seed, scale);
     else
-        k_generate_G<float><<<blocks_for(4LL * V, 128), 128, 0, ctx->stream>>>((cplx<float>*)b.U[0], V, seed, scale);
+        k_generate_G<float><<<blocks_for(4LL * V, 128), 128, 0, st>>>((cplx<float>*)b.U[0], V, seed, scale);
     LGF_CUDA_TRY(ctx, cudaGetLastError());
     return LGF_OK;
+}
+
+int launch_generate(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale) {
+    return launch_generate_on(ctx, b, seed, scale, ctx->stream);
 }
 
 int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b) {
@@ -609,12 +714,12 @@ void release_pinned_chunks(lgf_ctx* ctx) {
     }
 }
 
-int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host) {
+int upload_links_on(lgf_ctx* ctx, LatticeBuf& b, const double* host, cudaStream_t st) {
     const size_t bytes = (size_t)b.g.V * 4 * 18 * sizeof(double);
     char* stage = (char*)file_staging(b);
     cudaError_t e = cudaSuccess;
     if (is_pinned(host)) {
-        e = cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, st);
     } else {
         std::lock_guard<std::mutex> lk(ctx->pin_mu);
         e = ensure_pinned_chunks(ctx);
@@ -622,20 +727,25 @@ int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host) {
             cudaGetLastError();
             return set_error(ctx, LGF_ENOMEM, "pinned staging allocation failed: %s", cudaGetErrorString(e));
         }
+        // a chunk is refilled only after the DMA that last read it (on
+        // whichever stream) has finished: its event
         for (size_t off = 0, i = 0; off < bytes && e == cudaSuccess; off += PIN_CHUNK, ++i) {
             const size_t n = std::min(PIN_CHUNK, bytes - off);
             const int k = (int)(i & 1);
-            e = cudaEventSynchronize(ctx->pin_done[k]);  // the DMA that last read chunk k has finished
+            e = cudaEventSynchronize(ctx->pin_done[k]);
             if (e != cudaSuccess) break;
             std::memcpy(ctx->pin[k], (const char*)host + off, n);
-            e = cudaMemcpyAsync(stage + off, ctx->pin[k], n, cudaMemcpyHostToDevice, ctx->stream);
-            if (e == cudaSuccess) e = cudaEventRecord(ctx->pin_done[k], ctx->stream);
+            e = cudaMemcpyAsync(stage + off, ctx->pin[k], n, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->pin_done[k], st);
         }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // chunks free for the next caller
     }
     if (e != cudaSuccess) return set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
-    int rc = launch_to_device(ctx, b, (const double*)stage);
-    e = cudaStreamSynchronize(ctx->stream);
+    return launch_to_device_on(ctx, b, (const double*)stage, st);
+}
+
+int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host) {
+    int rc = upload_links_on(ctx, b, host, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (rc == LGF_OK && e != cudaSuccess) rc = set_error(ctx, LGF_ECUDA, "upload failed: %s", cudaGetErrorString(e));
     return rc;
 }
@@ -827,17 +937,17 @@ int lgf_generate_links(lgf_lattice* lat, uint64_t seed, double scale) {
 
 static int lattice_group(lgf_lattice* lat, GroupBase** out) {
     lgf_ctx* ctx = lat->ctx;
-    const int threads = stage_threads(ctx, lat->buf.prec, lat->buf.g.V);
-    if (lat->group && lat->group_threads != threads) {
+    const TileShape shape = tuned_shape(ctx, lat->buf.prec, lat->buf.g.V);
+    if (lat->group && lat->group_shape != shape) {
         cudaStreamSynchronize(ctx->stream);
         delete lat->group;
         lat->group = nullptr;
     }
     if (!lat->group) {
-        const long long ntiles = (4LL * lat->buf.g.V + threads - 1) / threads;
-        lat->group = make_group(ctx, lat->buf.prec, threads, 1, ntiles, false);
+        const long long ntiles = (4LL * lat->buf.g.V + shape.threads - 1) / shape.threads;
+        lat->group = make_group(ctx, lat->buf.prec, shape, 1, ntiles, false);
         if (!lat->group) return ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
-        lat->group_threads = threads;
+        lat->group_shape = shape;
         std::vector<LatticeBuf*> m{&lat->buf};
         int rc = lat->group->set_members(m);
         if (rc != LGF_OK) return rc;

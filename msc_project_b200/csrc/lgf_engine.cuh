@@ -28,14 +28,33 @@ struct NvtxRange {
 };
 #endif
 
+namespace lgf {
+// Launch shapes and work orders of a group's kernels, chosen per (precision,
+// volume class) by the autotuner.  Every choice gives the same results bit
+// for bit: only the block shapes and the order of the tiles change (no
+// reduction runs in tile order).
+struct TileShape {
+    int threads = 256;            // stage block size: a multiple of 128, at most LGF_STAGE_MAXT
+    int stage_order = 1;          // 0: blocks of x1 rows swept through x0; 1: x1 columns per CTA
+    double stage_budget = 8.0 * (1 << 20);  // blocked order: stage bytes per row block and slice
+    double meas_budget = 2.0 * (1 << 20);   // measurement: link bytes per row block and slice
+    int meas_split = 2;           // measurement warps per plane (1: 6-warp blocks, 2: 12-warp blocks)
+    bool operator==(const TileShape& o) const {
+        return threads == o.threads && stage_order == o.stage_order && stage_budget == o.stage_budget &&
+               meas_budget == o.meas_budget && meas_split == o.meas_split;
+    }
+    bool operator!=(const TileShape& o) const { return !(*this == o); }
+};
+}  // namespace lgf
+
 struct lgf_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     std::string err;
-    // autotuned stage block sizes: (precision, lattice volume, threads); a
-    // result applies to volumes within a factor of two of the tuned one
-    struct Tuned { int prec; long long volume; int threads; };
+    // autotuned tile shapes: (precision, lattice volume, shape); a result
+    // applies to volumes within a factor of two of the tuned one
+    struct Tuned { int prec; long long volume; lgf::TileShape shape; };
     std::vector<Tuned> tuned;
     // two pinned host chunks for uploads/downloads from pageable memory
     // (allocated on first use; a server's worker shares them, hence the lock)
@@ -58,9 +77,13 @@ int set_error(lgf_ctx* ctx, int code, const char* fmt, ...);
 bool valid_shape(const int shape[4]);
 size_t footprint_bytes(const int shape[4], int precision, int meas_slots);
 int default_threads(int precision);
-// the tuned block size for a lattice of this precision and volume, else the default
-int stage_threads(const lgf_ctx* ctx, int precision, long long volume);
-void record_tuned(lgf_ctx* ctx, int precision, long long volume, int threads);
+TileShape default_shape(int precision);
+// the tuned shape for a lattice of this precision and volume, else the default
+TileShape tuned_shape(const lgf_ctx* ctx, int precision, long long volume);
+bool has_tuned(const lgf_ctx* ctx, int precision, long long volume);
+void record_tuned(lgf_ctx* ctx, int precision, long long volume, const TileShape& shape);
+// times the candidate shapes on a lattice of this shape; the fastest is recorded and returned
+int tune_shape(lgf_ctx* ctx, int precision, const int shape[4], TileShape* best);
 
 // Device resources of one lattice (precision-erased).
 struct LatticeBuf {
@@ -75,9 +98,13 @@ struct LatticeBuf {
     int* slot = nullptr;
     int nchunk = 0;
     double eps = 0.0;
+    bool placed = false;  // laid out in caller memory (buf_place): buf_free does not free it
 };
 
 int buf_alloc(lgf_ctx* ctx, LatticeBuf& b, const int shape[4], int precision, int meas_slots);
+// bytes of one block holding a lattice's buffers, and their layout inside such a block
+size_t placed_bytes(const int shape[4], int precision, int meas_slots);
+void buf_place(LatticeBuf& b, const int shape[4], int precision, int meas_slots, void* mem);
 int buf_grow_meas(lgf_ctx* ctx, LatticeBuf& b, int meas_slots);
 void buf_free(LatticeBuf& b);
 
@@ -101,17 +128,24 @@ public:
     virtual int replay_measure() = 0;
     virtual int launches_per_step() const = 0;
     virtual int threads() const = 0;
+    virtual const TileShape& shape() const = 0;
 };
 
-GroupBase* make_group(lgf_ctx* ctx, int precision, int threads, int max_members, long long max_tiles, bool dynamic);
+GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
+                      bool dynamic);
 
 int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b);
 int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file_order);
 int launch_to_file(lgf_ctx* ctx, const LatticeBuf& b, double* dev_file_order);
 int launch_generate(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale);
+int launch_generate_on(lgf_ctx* ctx, LatticeBuf& b, unsigned long long seed, double scale, cudaStream_t st);
 
 // host<->device copies of file-order links, staged in the lattice's ring
 int upload_links(lgf_ctx* ctx, LatticeBuf& b, const double* host);
+// the same, enqueued on stream st without waiting for it: page-locked host
+// memory is read by the DMA later (keep it valid until st gets there);
+// pageable memory has been copied to the context's pinned chunks on return
+int upload_links_on(lgf_ctx* ctx, LatticeBuf& b, const double* host, cudaStream_t st);
 int download_links(lgf_ctx* ctx, const LatticeBuf& b, double* host);
 void release_pinned_chunks(lgf_ctx* ctx);
 
@@ -128,7 +162,7 @@ struct lgf_lattice {
     lgf_ctx* ctx = nullptr;
     lgf::LatticeBuf buf;
     lgf::GroupBase* group = nullptr;  // single-member group, created on first flow
-    int group_threads = 0;
+    lgf::TileShape group_shape;
     double last_flow_s = 0.0;
     unsigned long long hb_epoch = 0;  // heatbath random-number stream position
 };

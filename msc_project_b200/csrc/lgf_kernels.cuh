@@ -33,13 +33,7 @@
 #define LGF_STAGE_MINB 1
 #endif
 #ifndef LGF_MEAS_QSPLIT
-#define LGF_MEAS_QSPLIT 2  // measurement warps per plane (the four quadrants split between them)
-#endif
-#ifndef LGF_MEAS_MINB_D
-#define LGF_MEAS_MINB_D (LGF_MEAS_QSPLIT == 2 ? 1 : 2)  // double: resident measurement blocks per SM (caps registers)
-#endif
-#ifndef LGF_MEAS_MINB_F
-#define LGF_MEAS_MINB_F (LGF_MEAS_QSPLIT == 2 ? 1 : 2)  // float
+#define LGF_MEAS_QSPLIT 2  // default measurement warps per plane (the four quadrants split between them)
 #endif
 
 namespace lgf {
@@ -79,10 +73,88 @@ __device__ __forceinline__ su3<R> staple_sum(const cplx<R>* __restrict__ U, cons
     return S;
 }
 
+// The same staple sum with each term built row by row from the left: row r
+// of U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag and of
+// U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu) as a row vector times two
+// matrices, so no 3x3 intermediate is held (the same 54 complex multiply-adds
+// per term; only the association differs, which changes rounding only).
+template <typename R>
+__device__ __forceinline__ su3<R> staple_sum_rows(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                                  int mu) {
+    const int V = g.V;
+    const Dir dm = dir_of(g, c, mu);
+    su3<R> S;
+    su3_zero(S);
+    const int xpm = fwd(s, dm);
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        const int xpn = fwd(g, s, nu, c.x[nu]);
+        const int xmn = bwd(g, s, nu, c.x[nu]);
+        const int xmnpm = fwd(xmn, dm);
+        {
+            const su3<R> a3 = load_link(U, V, mu, xpn);
+            const su3<R> a2 = load_link(U, V, nu, s);
+            const cplx<R>* a1p = U + link_offset(nu, 0, xpm);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                cplx<R> a1r[3], v[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) a1r[j] = ldc(a1p + (3 * r + j) * LAYOUT_BLOCK);
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {  // v = a1[r,:] a3^dag
+                    cplx<R> t = cmulc(a1r[0], a3.m[3 * cc]);
+                    t = cfmac(a1r[1], a3.m[3 * cc + 1], t);
+                    v[cc] = cfmac(a1r[2], a3.m[3 * cc + 2], t);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {  // S[r,:] += v a2^dag
+                    cplx<R> t = S.m[3 * r + cc];
+                    t = cfmac(v[0], a2.m[3 * cc], t);
+                    t = cfmac(v[1], a2.m[3 * cc + 1], t);
+                    S.m[3 * r + cc] = cfmac(v[2], a2.m[3 * cc + 2], t);
+                }
+            }
+        }
+        {
+            const su3<R> b1 = load_link(U, V, mu, xmn);
+            const su3<R> b3 = load_link(U, V, nu, xmn);
+            const cplx<R>* b2p = U + link_offset(nu, 0, xmnpm);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                cplx<R> u[3], v[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {  // row r of b2^dag: conj of column r of b2
+                    const cplx<R> z = ldc(b2p + (3 * j + r) * LAYOUT_BLOCK);
+                    u[j] = cmk<R>(z.re, -z.im);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {  // v = u b1^dag
+                    cplx<R> t = cmulc(u[0], b1.m[3 * cc]);
+                    t = cfmac(u[1], b1.m[3 * cc + 1], t);
+                    v[cc] = cfmac(u[2], b1.m[3 * cc + 2], t);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {  // S[r,:] += v b3
+                    cplx<R> t = S.m[3 * r + cc];
+                    t = cfma(v[0], b3.m[cc], t);
+                    t = cfma(v[1], b3.m[3 + cc], t);
+                    S.m[3 * r + cc] = cfma(v[2], b3.m[6 + cc], t);
+                }
+            }
+        }
+    }
+    return S;
+}
+
+#ifndef LGF_STAPLE_ROWS
+#define LGF_STAPLE_ROWS 0  // 1: build the staple terms row by row (staple_sum_rows)
+#endif
+
 template <typename R>
 __device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                 int mu, su3<R>& u_out) {
-    const su3<R> S = staple_sum<R>(U, g, s, c, mu);
+    const su3<R> S = LGF_STAPLE_ROWS ? staple_sum_rows<R>(U, g, s, c, mu) : staple_sum<R>(U, g, s, c, mu);
     u_out = load_link(U, g.V, mu, s);
     const su3<R> W = mul_nn(u_out, S);
     return ta_part(W, R(-0.5));
@@ -199,7 +271,7 @@ template <typename R> struct Plane {
         return a;
     }
     // move p by count steps without loading links
-    __device__ __forceinline__ void advance(PlanePos& p, bool along_mu, int sign, int count) const {
+    __host__ __device__ __forceinline__ void advance(PlanePos& p, bool along_mu, int sign, int count) const {
         const Dir& d = along_mu ? dm : dn;
         int& xc = along_mu ? p.xm : p.xn;
         for (int i = 0; i < count; ++i) {
@@ -294,6 +366,9 @@ __device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
 constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
 constexpr int MEAS_QSPLIT = LGF_MEAS_QSPLIT;
 constexpr int MEAS_WARPS = 6 * MEAS_QSPLIT;  // warp y: plane y % 6, quadrants of part y / 6
+// resident measurement blocks per SM the launch bounds ask for (caps the
+// registers): one block of 12 warps with the quadrants split, else two of 6
+template <int QS> struct MeasMinBlocks { static constexpr int value = QS == 2 ? 1 : 2; };
 
 // Shared memory of one measurement block: the straight lines of length 2 and
 // 3 from each of its 32 sites in the 8 signed directions (every plane and
@@ -432,9 +507,10 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
 }
 
 // Measurement tile = (lattice, x0 slice, chunk of 32 consecutive sites of the
-// slice); 6 x MEAS_QSPLIT warps: warp y takes plane y % 6 and the quadrants
-// of part y / 6.  Phase 0: the block's lines (warp w builds the lines of
-// signed direction w, w + MEAS_WARPS, ...) into shared memory.  Phase 1: the
+// slice); 6 x QS warps: warp y takes plane y % 6 and the quadrants of part
+// y / 6 (QS = 1: all four; QS = 2: two each).  Phase 0: the block's lines
+// (warp w builds the lines of signed direction w, w + 6 QS, ...) into shared
+// memory.  Phase 1: the
 // quadrant sums of every (site, plane); with two parts the second part's sums
 // meet the first's in the (then dead) line storage, in a fixed order, for F
 // and F^.  Phase 2: the six planes meet in shared
@@ -446,18 +522,16 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
 //   q(x) = ReTr(F^32 F^01) + ReTr(F^31 F^20) + ReTr(F^30 F^12)
 //        = -T(23,01) + T(13,02) - T(03,12),  T(a,b) = ReTr(F^a F^b)
 //                                             (TopologicalCharge.cpp:11-16)
-template <typename R> struct MeasMinBlocks { static constexpr int value = LGF_MEAS_MINB_F; };
-template <> struct MeasMinBlocks<double> { static constexpr int value = LGF_MEAS_MINB_D; };
-
-template <typename R, bool OUT = false>
-__global__ void __launch_bounds__(MEAS_SITES * MEAS_WARPS, MeasMinBlocks<R>::value) k_measure(const LatDesc<R>* __restrict__ descs,
+template <typename R, bool OUT = false, int QS = MEAS_QSPLIT>
+__global__ void __launch_bounds__(MEAS_SITES * 6 * QS, MeasMinBlocks<QS>::value) k_measure(const LatDesc<R>* __restrict__ descs,
                                                                            const int4* __restrict__ mtiles,
                                                                            const int* __restrict__ nmtiles,
                                                                            MeasOut out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MeasSmem<R, OUT>* sm = reinterpret_cast<MeasSmem<R, OUT>*>(smem_raw);
     const int lane = threadIdx.x, w = threadIdx.y, p = w % 6, part = w / 6;
-    const int qa = part * (4 / MEAS_QSPLIT), qb = qa + 4 / MEAS_QSPLIT;
+    constexpr int NW = 6 * QS;  // warps of the block
+    const int qa = part * (4 / QS), qb = qa + 4 / QS;
     const int n = *nmtiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
         const int4 tile = mtiles[ti];
@@ -470,7 +544,7 @@ __global__ void __launch_bounds__(MEAS_SITES * MEAS_WARPS, MeasMinBlocks<R>::val
         const Coord c = site_coord(g, s);
         const cplx<R>* __restrict__ U = d->U0;
         // phase 0: lines of length 2 and 3 in the 8 signed directions
-        for (int sdir = w; sdir < 8; sdir += MEAS_WARPS) {
+        for (int sdir = w; sdir < 8; sdir += NW) {
             const int dir = sdir >> 1, sign = (sdir & 1) ? -1 : 1;
             Plane<R> L;
             L.U = U;
@@ -490,7 +564,7 @@ __global__ void __launch_bounds__(MEAS_SITES * MEAS_WARPS, MeasMinBlocks<R>::val
         // phase 1: this thread's plane and quadrants
         alg<R> G, Fh;
         if (valid) plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, qa, qb, G, Fh);
-        if (MEAS_QSPLIT == 2) {
+        if (QS == 2) {
             __syncthreads();  // every warp is done with the lines
             if (part == 1 && valid) {
                 sm->part.G[p][lane] = G;
@@ -556,8 +630,8 @@ __global__ void __launch_bounds__(MEAS_SITES * MEAS_WARPS, MeasMinBlocks<R>::val
 // Dynamic shared memory of k_measure<R> (above 48 KB for double: the
 // attribute must be raised once per device before the first launch).
 template <typename R, bool OUT = false> inline size_t measure_smem_bytes() { return sizeof(MeasSmem<R, OUT>); }
-template <typename R, bool OUT = false> inline cudaError_t prepare_measure_kernel() {
-    return cudaFuncSetAttribute(k_measure<R, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <typename R, bool OUT = false, int QS = MEAS_QSPLIT> inline cudaError_t prepare_measure_kernel() {
+    return cudaFuncSetAttribute(k_measure<R, OUT, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(MeasSmem<R, OUT>));
 }
 

@@ -19,6 +19,23 @@
 #include <stdint.h>
 #include "lgf_su3.cuh"
 
+// -DLGF_CHECKED: host-side uses of the index arithmetic assert that every
+// coordinate, direction and site index stays in range (the CPU index check,
+// lgf_check_index.cu); device code is unchanged.
+#if defined(LGF_CHECKED) && !defined(__CUDA_ARCH__)
+#include <cstdio>
+#include <cstdlib>
+#define LGF_INDEX_ASSERT(cond)                                                                      \
+    do {                                                                                            \
+        if (!(cond)) {                                                                              \
+            std::fprintf(stderr, "LGF_CHECKED: index check failed: %s (%s:%d)\n", #cond, __FILE__, __LINE__); \
+            std::abort();                                                                           \
+        }                                                                                           \
+    } while (0)
+#else
+#define LGF_INDEX_ASSERT(cond) ((void)0)
+#endif
+
 namespace lgf {
 
 struct Geom {
@@ -42,7 +59,8 @@ inline Geom make_geom(const int shape[4]) {
 
 struct Coord { int x[4]; };
 
-__device__ __forceinline__ Coord site_coord(const Geom& g, int s) {
+__host__ __device__ __forceinline__ Coord site_coord(const Geom& g, int s) {
+    LGF_INDEX_ASSERT(s >= 0 && s < g.V);
     Coord c;
     unsigned r = (unsigned)s;
     c.x[3] = (int)(r % (unsigned)g.n[3]); r /= (unsigned)g.n[3];
@@ -53,32 +71,45 @@ __device__ __forceinline__ Coord site_coord(const Geom& g, int s) {
 }
 
 // index of the neighbour of s (whose d-coordinate is xd) one step forward / back in d
-__device__ __forceinline__ int fwd(const Geom& g, int s, int d, int xd) {
-    return (xd == g.n[d] - 1) ? s - (g.n[d] - 1) * g.stride[d] : s + g.stride[d];
+__host__ __device__ __forceinline__ int fwd(const Geom& g, int s, int d, int xd) {
+    LGF_INDEX_ASSERT(d >= 0 && d < 4 && xd >= 0 && xd < g.n[d] && s >= 0 && s < g.V);
+    const int r = (xd == g.n[d] - 1) ? s - (g.n[d] - 1) * g.stride[d] : s + g.stride[d];
+    LGF_INDEX_ASSERT(r >= 0 && r < g.V);
+    return r;
 }
-__device__ __forceinline__ int bwd(const Geom& g, int s, int d, int xd) {
-    return (xd == 0) ? s + (g.n[d] - 1) * g.stride[d] : s - g.stride[d];
+__host__ __device__ __forceinline__ int bwd(const Geom& g, int s, int d, int xd) {
+    LGF_INDEX_ASSERT(d >= 0 && d < 4 && xd >= 0 && xd < g.n[d] && s >= 0 && s < g.V);
+    const int r = (xd == 0) ? s + (g.n[d] - 1) * g.stride[d] : s - g.stride[d];
+    LGF_INDEX_ASSERT(r >= 0 && r < g.V);
+    return r;
 }
-__device__ __forceinline__ int wrap_inc(int x, int n) { return x == n - 1 ? 0 : x + 1; }
-__device__ __forceinline__ int wrap_dec(int x, int n) { return x == 0 ? n - 1 : x - 1; }
+__host__ __device__ __forceinline__ int wrap_inc(int x, int n) { return x == n - 1 ? 0 : x + 1; }
+__host__ __device__ __forceinline__ int wrap_dec(int x, int n) { return x == 0 ? n - 1 : x - 1; }
 
 // One lattice direction as plain scalars (extent, stride, and the thread's
 // coordinate along it).  Selected without indexing a local array, so nothing
 // spills to local memory when the direction is only known at run time.
 struct Dir { int n, stride, x; };
 
-__device__ __forceinline__ int sel4(int d, int a0, int a1, int a2, int a3) {
+__host__ __device__ __forceinline__ int sel4(int d, int a0, int a1, int a2, int a3) {
     return d == 0 ? a0 : (d == 1 ? a1 : (d == 2 ? a2 : a3));
 }
-__device__ __forceinline__ Dir dir_of(const Geom& g, const Coord& c, int d) {
+__host__ __device__ __forceinline__ Dir dir_of(const Geom& g, const Coord& c, int d) {
+    LGF_INDEX_ASSERT(d >= 0 && d < 4);
     Dir r;
     r.n = sel4(d, g.n[0], g.n[1], g.n[2], g.n[3]);
     r.stride = sel4(d, g.stride[0], g.stride[1], g.stride[2], g.stride[3]);
     r.x = sel4(d, c.x[0], c.x[1], c.x[2], c.x[3]);
     return r;
 }
-__device__ __forceinline__ int fwd(int s, const Dir& d) { return (d.x == d.n - 1) ? s - (d.n - 1) * d.stride : s + d.stride; }
-__device__ __forceinline__ int bwd(int s, const Dir& d) { return (d.x == 0) ? s + (d.n - 1) * d.stride : s - d.stride; }
+__host__ __device__ __forceinline__ int fwd(int s, const Dir& d) {
+    LGF_INDEX_ASSERT(d.x >= 0 && d.x < d.n && s >= 0);
+    return (d.x == d.n - 1) ? s - (d.n - 1) * d.stride : s + d.stride;
+}
+__host__ __device__ __forceinline__ int bwd(int s, const Dir& d) {
+    LGF_INDEX_ASSERT(d.x >= 0 && d.x < d.n && s >= 0);
+    return (d.x == 0) ? s + (d.n - 1) * d.stride : s - d.stride;
+}
 
 template <typename R> struct vec2_of;
 template <> struct vec2_of<double> { typedef double2 type; };
@@ -104,9 +135,11 @@ constexpr int LAYOUT_BLOCK = LGF_LAYOUT_BLOCK;  // sites per layout block
 __host__ __device__ __forceinline__ size_t padded_sites(size_t V) { return (V + LAYOUT_BLOCK - 1) / LAYOUT_BLOCK * LAYOUT_BLOCK; }
 // offset of complex entry k of link mu at site s; entry k+1 is LAYOUT_BLOCK further
 __host__ __device__ __forceinline__ size_t link_offset(int mu, int k, int s) {
+    LGF_INDEX_ASSERT(mu >= 0 && mu < 4 && k >= 0 && k < 9 && s >= 0);
     return ((size_t)(s / LAYOUT_BLOCK) * 36 + mu * 9 + k) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
 }
 __host__ __device__ __forceinline__ size_t alg_offset(int mu, int c, int s) {
+    LGF_INDEX_ASSERT(mu >= 0 && mu < 4 && c >= 0 && c < 8 && s >= 0);
     return ((size_t)(s / LAYOUT_BLOCK) * 32 + mu * 8 + c) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
 }
 

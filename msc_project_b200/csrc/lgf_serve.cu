@@ -7,14 +7,24 @@
 // persistent launches (one group per precision, graph-captured once; the work
 // list and its length live in device memory so members join and leave without
 // re-capture), (3) measures the jobs that are due, and (4) retires finished
-// jobs: results are copied to the caller's arrays, device memory is released
-// and waiters are woken.  A job's arithmetic does not depend on which other
-// jobs share its launches, so its results are the same alone and in the mix.
+// jobs: results are copied to the caller's arrays, their memory returns to the
+// arena and waiters are woken.  A job's arithmetic does not depend on which
+// other jobs share its launches, so its results are the same alone and in the
+// mix.
+//
+// Memory: lgf_serve_start reserves the whole budget as one device arena, and
+// every job's buffers are one block of it (first fit, neighbouring free blocks
+// merged), so admission and retirement make no cudaMalloc / cudaFree (both of
+// which would stall the device).  Admission is asynchronous: a job's upload or
+// generation runs on a second stream, after the retirements whose memory it
+// may reuse (an event), and the job joins the shared launches once its own
+// event reports the input in place; resident jobs keep flowing meanwhile.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -36,11 +46,69 @@ struct ServeJob {
     lgf_job job{};
     lgf_job_status st{};
     size_t bytes = 0;
+    char* mem = nullptr;             // its block of the arena while admitted
+    cudaEvent_t ready = nullptr;     // its input is in place (admission stream)
     LatticeBuf buf;
     int nmeas = 0;
     std::atomic<int> steps_done{0};  // advanced by the worker, read by pollers
     double t = 0.0;
     std::vector<double> tvals;
+};
+
+// One device reservation carved into job blocks: first fit over a map of free
+// blocks (offset -> length), neighbours merged on release.  Used by the
+// scheduler thread only.
+class Arena {
+public:
+    ~Arena() {
+        if (base_) cudaFree(base_);
+    }
+    cudaError_t reserve(size_t bytes) {
+        cudaError_t e = cudaMalloc(&base_, bytes);
+        if (e != cudaSuccess) {
+            base_ = nullptr;
+            return e;
+        }
+        size_ = bytes;
+        free_[0] = bytes;
+        return cudaSuccess;
+    }
+    char* alloc(size_t n) {
+        n = round(n);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            const size_t off = it->first, len = it->second;
+            free_.erase(it);
+            if (len > n) free_[off + n] = len - n;
+            return base_ + off;
+        }
+        return nullptr;
+    }
+    void release(char* p, size_t n) {
+        n = round(n);
+        size_t off = (size_t)(p - base_);
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && off + n == next->first) {
+            n += next->second;
+            free_.erase(next);
+        }
+        auto prev = free_.lower_bound(off);
+        if (prev != free_.begin()) {
+            --prev;
+            if (prev->first + prev->second == off) {
+                off = prev->first;
+                n += prev->second;
+                free_.erase(prev);
+            }
+        }
+        free_[off] = n;
+    }
+
+private:
+    static size_t round(size_t n) { return (n + 255) & ~size_t(255); }
+    char* base_ = nullptr;
+    size_t size_ = 0;
+    std::map<size_t, size_t> free_;
 };
 
 double now_s(std::chrono::steady_clock::time_point t0) {
@@ -58,15 +126,19 @@ struct lgf_server {
     int waiters = 0;  // threads inside lgf_serve_wait; stop frees the server only when none is left
     std::deque<ServeJob*> queue;
     std::map<uint64_t, std::unique_ptr<ServeJob>> jobs;
+    std::vector<ServeJob*> staging;  // admitted, input still arriving
     std::vector<ServeJob*> active;
     size_t used = 0;
+    Arena arena;
+    cudaStream_t adm = nullptr;        // admission stream: uploads and generation
+    cudaEvent_t retired_ev = nullptr;  // recorded on the flow stream at each retirement
     uint64_t next_id = 1;
     bool stopping = false;
     std::thread worker;
     std::unique_ptr<GroupBase> group[2];
     std::vector<LatticeBuf*> members[2];  // current member list of each group
     std::vector<int> measured[2];         // current measured subset of each group
-    int threads[2] = {0, 0};
+    TileShape shape[2];
     long long max_tiles[2] = {0, 0};
     int fatal = LGF_OK;
 
@@ -78,6 +150,17 @@ struct lgf_server {
 };
 
 void lgf_server::finish(ServeJob* j, int state, int err) {
+    // the flow stream's work on this job's block is enqueued by now; a later
+    // admission that reuses the block waits for this point
+    if (j->mem) {
+        cudaEventRecord(retired_ev, ctx->stream);
+        arena.release(j->mem, j->bytes);
+        j->mem = nullptr;
+    }
+    if (j->ready) {
+        cudaEventDestroy(j->ready);
+        j->ready = nullptr;
+    }
     buf_free(j->buf);
     std::lock_guard<std::mutex> lk(mu);
     used -= j->bytes;
@@ -88,15 +171,19 @@ void lgf_server::finish(ServeJob* j, int state, int err) {
     cv_done.notify_all();
 }
 
+// Lay the job out in its arena block and enqueue its input on the admission
+// stream, behind the retirements whose memory the block may reuse.
 int lgf_server::admit(ServeJob* j) {
-    int rc = buf_alloc(ctx, j->buf, j->job.shape, j->job.precision, j->nmeas);
-    if (rc == LGF_OK)
-        rc = j->job.links ? upload_links(ctx, j->buf, j->job.links)
-                          : launch_generate(ctx, j->buf, j->job.seed, j->job.gen_scale);
+    buf_place(j->buf, j->job.shape, j->job.precision, j->nmeas, j->mem);
+    LGF_CUDA_TRY(ctx, cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming));
+    LGF_CUDA_TRY(ctx, cudaStreamWaitEvent(adm, retired_ev, 0));
+    int rc = j->job.links ? upload_links_on(ctx, j->buf, j->job.links, adm)
+                          : launch_generate_on(ctx, j->buf, j->job.seed, j->job.gen_scale, adm);
     if (rc != LGF_OK) return rc;
     j->buf.eps = j->job.flow.eps;
     j->t = j->job.flow.t0;
-    LGF_CUDA_TRY(ctx, cudaMemsetAsync(j->buf.slot, 0, sizeof(int), ctx->stream));
+    LGF_CUDA_TRY(ctx, cudaMemsetAsync(j->buf.slot, 0, sizeof(int), adm));
+    LGF_CUDA_TRY(ctx, cudaEventRecord(j->ready, adm));
     return LGF_OK;
 }
 
@@ -132,7 +219,7 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
     for (int p = 0; p < 2; ++p) {
         if (byprec[p].empty()) continue;
         if (!group[p]) {
-            group[p].reset(make_group(ctx, p, threads[p], std::max(cfg.max_active, 1), max_tiles[p], true));
+            group[p].reset(make_group(ctx, p, shape[p], std::max(cfg.max_active, 1), max_tiles[p], true));
             if (!group[p]) return LGF_ENOMEM;
         }
         std::vector<LatticeBuf*> m;
@@ -213,13 +300,16 @@ void lgf_server::run() {
         std::vector<ServeJob*> admitted;
         {
             std::unique_lock<std::mutex> lk(mu);
-            if (active.empty() && queue.empty() && !stopping)
+            if (active.empty() && staging.empty() && queue.empty() && !stopping)
                 cv_work.wait_for(lk, std::chrono::milliseconds(20));
             if (stopping) break;
-            // arrival-order admission by HBM footprint and free slots
-            while (!queue.empty() && (int)(active.size() + admitted.size()) < cfg.max_active &&
+            // arrival-order admission by HBM footprint, free slots and a free
+            // arena block (the head waits for retirements if none fits)
+            while (!queue.empty() && (int)(active.size() + staging.size() + admitted.size()) < cfg.max_active &&
                    used + queue.front()->bytes <= cfg.hbm_budget_bytes) {
                 ServeJob* j = queue.front();
+                j->mem = arena.alloc(j->bytes);
+                if (!j->mem) break;
                 queue.pop_front();
                 used += j->bytes;
                 j->st.state = LGF_JOB_RUNNING;
@@ -230,8 +320,24 @@ void lgf_server::run() {
         for (auto* j : admitted) {
             int rc = admit(j);
             if (rc != LGF_OK) finish(j, LGF_JOB_FAILED, rc);
-            else active.push_back(j);
+            else staging.push_back(j);
         }
+        // jobs whose input has arrived join the shared launches; with nothing
+        // else to run, wait for the first of them
+        if (active.empty() && !staging.empty()) cudaEventSynchronize(staging.front()->ready);
+        std::vector<ServeJob*> still;
+        for (auto* j : staging) {
+            const cudaError_t q = cudaEventQuery(j->ready);
+            if (q == cudaSuccess) {
+                active.push_back(j);
+            } else if (q == cudaErrorNotReady) {
+                still.push_back(j);
+            } else {
+                cudaGetLastError();
+                finish(j, LGF_JOB_FAILED, set_error(ctx, LGF_ECUDA, "job input failed: %s", cudaGetErrorString(q)));
+            }
+        }
+        staging.swap(still);
         if (active.empty()) continue;
         int rc = tick(active);
         if (rc != LGF_OK) {
@@ -251,10 +357,30 @@ void lgf_server::run() {
         active.swap(keep);
     }
     cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(adm);
+    for (auto* j : staging) finish(j, LGF_JOB_FAILED, LGF_ESHUTDOWN);
+    staging.clear();
     for (auto* j : active) finish(j, LGF_JOB_FAILED, LGF_ESHUTDOWN);
     active.clear();
     group[0].reset();
     group[1].reset();
+}
+
+// Tile shape for the shared launches of one precision: the tuned shape of the
+// context's tuned volume nearest to 2^20 sites (the middle of the served
+// volumes), else the default.
+static TileShape serve_shape(const lgf_ctx* ctx, int prec) {
+    TileShape best = default_shape(prec);
+    double dist = 1e300;
+    for (const auto& t : ctx->tuned) {
+        if (t.prec != prec) continue;
+        const double d = std::fabs(std::log((double)t.volume / (double)(1 << 20)));
+        if (d < dist) {
+            dist = d;
+            best = t.shape;
+        }
+    }
+    return best;
 }
 
 extern "C" {
@@ -270,12 +396,26 @@ int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out)
     s->cfg = *cfg;
     if (s->cfg.steps_per_tick < 1) s->cfg.steps_per_tick = 1;
     s->t0 = std::chrono::steady_clock::now();
+    cudaError_t e = s->arena.reserve(cfg->hbm_budget_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return set_error(ctx, LGF_ENOMEM, "cannot reserve the %zu-byte serving budget: %s", cfg->hbm_budget_bytes,
+                         cudaGetErrorString(e));
+    }
+    if (cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->retired_ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->adm) cudaStreamDestroy(s->adm);
+        delete s;
+        return set_error(ctx, LGF_ECUDA, "cannot create the admission stream");
+    }
     for (int p = 0; p < 2; ++p) {
-        s->threads[p] = default_threads(p);  // jobs of every volume share the server's launches
+        s->shape[p] = serve_shape(ctx, p);  // jobs of every volume share the server's launches
         // the budget bounds the resident sites: every site costs at least its links ring + accumulator
         const size_t per_site = (p == 0 ? 8 : 4) * (3 * 4 * 18 + 4 * 8);
         const long long max_sites = (long long)(cfg->hbm_budget_bytes / per_site) + 1;
-        s->max_tiles[p] = (4 * max_sites) / s->threads[p] + 2LL * cfg->max_active + 1;
+        s->max_tiles[p] = (4 * max_sites) / s->shape[p].threads + 2LL * cfg->max_active + 1;
     }
     s->worker = std::thread([s] { s->run(); });
     *out = s;
@@ -293,7 +433,7 @@ int lgf_serve_submit(lgf_server* s, const lgf_job* job, uint64_t* id) {
     auto j = std::make_unique<ServeJob>();
     j->job = *job;
     j->nmeas = nm;
-    j->bytes = footprint_bytes(job->shape, job->precision, nm);
+    j->bytes = placed_bytes(job->shape, job->precision, nm);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) return LGF_ESHUTDOWN;
     if (j->bytes > s->cfg.hbm_budget_bytes) return LGF_ENOMEM;  // could never be admitted
@@ -358,6 +498,8 @@ int lgf_serve_stop(lgf_server* s) {
         s->cv_done.notify_all();
         s->cv_idle.wait(lk, [s] { return s->waiters == 0; });
     }
+    cudaEventDestroy(s->retired_ev);
+    cudaStreamDestroy(s->adm);
     delete s;
     return LGF_OK;
 }

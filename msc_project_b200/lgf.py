@@ -109,6 +109,26 @@ class Context:
         self.check(self.lib.lgf_autotune(self.h, precision_code(precision), _shape(shape), ctypes.byref(best)))
         return best.value
 
+    def autotune_tiles(self, precision, shape) -> dict:
+        """Tune the stage and measurement tile shapes for this volume class; returns the choice."""
+        t = C.lgf_tile_shape()
+        self.check(self.lib.lgf_autotune_tiles(self.h, precision_code(precision), _shape(shape), ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in C.lgf_tile_shape._fields_}
+
+    def set_tiles(self, precision, shape, **tiles):
+        """Fix the tile shape of this precision and volume class (fields of lgf_tile_shape)."""
+        t = C.lgf_tile_shape()
+        cur = self.get_tiles(precision, shape)
+        cur.update(tiles)
+        for f, _ in C.lgf_tile_shape._fields_:
+            setattr(t, f, int(cur[f]))
+        self.check(self.lib.lgf_set_tiles(self.h, precision_code(precision), _shape(shape), ctypes.byref(t)))
+
+    def get_tiles(self, precision, shape) -> dict:
+        t = C.lgf_tile_shape()
+        self.check(self.lib.lgf_get_tiles(self.h, precision_code(precision), _shape(shape), ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in C.lgf_tile_shape._fields_}
+
     def batch_run(self, jobs: list["Job"]) -> C.lgf_batch_stats:
         arr = (C.lgf_job * len(jobs))()
         for i, j in enumerate(jobs):
