@@ -184,6 +184,12 @@ typedef struct lgf_job {
     lgf_flow_opts flow;     /* eps, nsteps, meas_every, t0, measure_at_t0, reunit_every */
     lgf_meas* meas;         /* results (may be NULL) */
     double* links_out;      /* optional: final links, file order */
+    /* serving only (ignored by lgf_batch_run): when not NULL, the links after
+     * each measured RK3 step are written to <snapshot_prefix>_Flowtime<t>.bin,
+     * t formatted like the reference's saved flowed configurations
+     * (std::to_string, LGF/LGF.cpp:194) in the same file layout, so a job can
+     * be resumed from its last snapshot (links = file, flow.t0 = t) */
+    const char* snapshot_prefix;
 } lgf_job;
 
 typedef struct lgf_batch_stats {

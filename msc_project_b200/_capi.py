@@ -43,7 +43,7 @@ class lgf_flow_opts(ctypes.Structure):
 class lgf_job(ctypes.Structure):
     _fields_ = [("shape", ctypes.c_int * 4), ("precision", ctypes.c_int), ("links", _dp), ("seed", ctypes.c_uint64),
                 ("gen_scale", ctypes.c_double), ("flow", lgf_flow_opts), ("meas", ctypes.POINTER(lgf_meas)),
-                ("links_out", _dp)]
+                ("links_out", _dp), ("snapshot_prefix", ctypes.c_char_p)]
 
 
 class lgf_batch_stats(ctypes.Structure):

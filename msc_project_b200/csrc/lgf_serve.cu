@@ -19,6 +19,13 @@
 // generation runs on a second stream, after the retirements whose memory it
 // may reuse (an event), and the job joins the shared launches once its own
 // event reports the input in place; resident jobs keep flowing meanwhile.
+//
+// Snapshots: a job with a snapshot prefix gets, after each measured step, its
+// links reordered to file order into a buffer of its own block (on the flow
+// stream); a writer thread copies that buffer to the host on a third stream
+// once an event says it is complete and writes <prefix>_Flowtime<t>.bin, so
+// the flow never waits for the disk (only for a job's previous snapshot,
+// should it still be in flight).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,8 +34,10 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <cstdio>
 #include <deque>
 #include <map>
+#include <string>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -48,6 +57,9 @@ struct ServeJob {
     size_t bytes = 0;
     char* mem = nullptr;             // its block of the arena while admitted
     cudaEvent_t ready = nullptr;     // its input is in place (admission stream)
+    double* snap_buf = nullptr;      // file-order snapshot buffer (inside its block), or null
+    bool snap_pending = false;       // a snapshot of this job is being written (guarded by snap_mu)
+    int snap_err = LGF_OK;           // first failed snapshot write
     LatticeBuf buf;
     int nmeas = 0;
     std::atomic<int> steps_done{0};  // advanced by the worker, read by pollers
@@ -111,6 +123,17 @@ private:
     std::map<size_t, size_t> free_;
 };
 
+struct SnapTask {
+    ServeJob* job;
+    cudaEvent_t ev;  // the snapshot buffer is complete (flow stream)
+    std::string path;
+    size_t bytes;
+};
+
+size_t snapshot_bytes(const int shape[4]) {
+    return (size_t)shape[0] * shape[1] * shape[2] * shape[3] * 4 * 18 * sizeof(double);
+}
+
 double now_s(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -132,6 +155,13 @@ struct lgf_server {
     Arena arena;
     cudaStream_t adm = nullptr;        // admission stream: uploads and generation
     cudaEvent_t retired_ev = nullptr;  // recorded on the flow stream at each retirement
+    // snapshot writer
+    std::thread snap_thread;
+    cudaStream_t snap_stream = nullptr;
+    std::mutex snap_mu;
+    std::condition_variable snap_cv, snap_done_cv;
+    std::deque<SnapTask> snap_q;
+    bool snap_stop = false;
     uint64_t next_id = 1;
     bool stopping = false;
     std::thread worker;
@@ -143,13 +173,79 @@ struct lgf_server {
     int fatal = LGF_OK;
 
     void run();
+    void snap_run();
+    int snapshot(ServeJob* j);
+    void wait_snapshot(ServeJob* j);
     int tick(std::vector<ServeJob*>& act);
     int admit(ServeJob* j);
     int retire(ServeJob* j);
     void finish(ServeJob* j, int state, int err);
 };
 
+// writer thread: one snapshot at a time, in the order they were taken
+void lgf_server::snap_run() {
+    cudaSetDevice(ctx->device);
+    std::vector<double> host;
+    for (;;) {
+        SnapTask t;
+        {
+            std::unique_lock<std::mutex> lk(snap_mu);
+            snap_cv.wait(lk, [&] { return snap_stop || !snap_q.empty(); });
+            if (snap_q.empty()) return;
+            t = snap_q.front();
+            snap_q.pop_front();
+        }
+        int rc = LGF_OK;
+        host.resize(t.bytes / sizeof(double));
+        cudaError_t e = cudaStreamWaitEvent(snap_stream, t.ev, 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), t.job->snap_buf, t.bytes, cudaMemcpyDeviceToHost, snap_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(snap_stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            rc = LGF_ECUDA;
+        } else {
+            FILE* f = std::fopen(t.path.c_str(), "wb");
+            const bool ok = f && std::fwrite(host.data(), 1, t.bytes, f) == t.bytes;
+            if (f && std::fclose(f) != 0) rc = LGF_EIO;
+            if (!ok) rc = LGF_EIO;
+        }
+        cudaEventDestroy(t.ev);
+        std::lock_guard<std::mutex> lk(snap_mu);
+        if (rc != LGF_OK && t.job->snap_err == LGF_OK) t.job->snap_err = rc;
+        t.job->snap_pending = false;
+        snap_done_cv.notify_all();
+    }
+}
+
+void lgf_server::wait_snapshot(ServeJob* j) {
+    std::unique_lock<std::mutex> lk(snap_mu);
+    snap_done_cv.wait(lk, [&] { return !j->snap_pending; });
+}
+
+// the job's current links (after a measured step) to its snapshot file
+int lgf_server::snapshot(ServeJob* j) {
+    wait_snapshot(j);  // the buffer holds the previous snapshot until it is written
+    int rc = launch_to_file(ctx, j->buf, j->snap_buf);
+    if (rc != LGF_OK) return rc;
+    SnapTask t;
+    t.job = j;
+    t.bytes = snapshot_bytes(j->job.shape);
+    t.path = std::string(j->job.snapshot_prefix) + "_Flowtime" + std::to_string(j->t) + ".bin";
+    LGF_CUDA_TRY(ctx, cudaEventCreateWithFlags(&t.ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(t.ev, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(t.ev);
+        return set_error(ctx, LGF_ECUDA, "snapshot event failed: %s", cudaGetErrorString(e));
+    }
+    std::lock_guard<std::mutex> lk(snap_mu);
+    j->snap_pending = true;
+    snap_q.push_back(t);
+    snap_cv.notify_one();
+    return LGF_OK;
+}
+
 void lgf_server::finish(ServeJob* j, int state, int err) {
+    wait_snapshot(j);  // its buffer lives in the job's block
     // the flow stream's work on this job's block is enqueued by now; a later
     // admission that reuses the block waits for this point
     if (j->mem) {
@@ -175,6 +271,7 @@ void lgf_server::finish(ServeJob* j, int state, int err) {
 // stream, behind the retirements whose memory the block may reuse.
 int lgf_server::admit(ServeJob* j) {
     buf_place(j->buf, j->job.shape, j->job.precision, j->nmeas, j->mem);
+    if (j->job.snapshot_prefix) j->snap_buf = (double*)(j->mem + placed_bytes(j->job.shape, j->job.precision, j->nmeas));
     LGF_CUDA_TRY(ctx, cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming));
     LGF_CUDA_TRY(ctx, cudaStreamWaitEvent(adm, retired_ev, 0));
     int rc = j->job.links ? upload_links_on(ctx, j->buf, j->job.links, adm)
@@ -288,6 +385,11 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
             if (!which.empty()) {
                 rc = measure(which);
                 if (rc != LGF_OK) return rc;
+                for (int i : which)
+                    if (run[i]->job.snapshot_prefix) {
+                        rc = snapshot(run[i]);
+                        if (rc != LGF_OK) return rc;
+                    }
             }
         }
     }
@@ -349,6 +451,8 @@ void lgf_server::run() {
         for (auto* j : active) {
             if (j->steps_done >= j->job.flow.nsteps) {
                 int r2 = retire(j);
+                wait_snapshot(j);
+                if (r2 == LGF_OK) r2 = j->snap_err;  // a snapshot that could not be written fails the job
                 finish(j, r2 == LGF_OK ? LGF_JOB_DONE : LGF_JOB_FAILED, r2);
             } else {
                 keep.push_back(j);
@@ -364,6 +468,12 @@ void lgf_server::run() {
     active.clear();
     group[0].reset();
     group[1].reset();
+    {
+        std::lock_guard<std::mutex> lk(snap_mu);
+        snap_stop = true;
+        snap_cv.notify_all();
+    }
+    if (snap_thread.joinable()) snap_thread.join();
 }
 
 // Tile shape for the shared launches of one precision: the tuned shape of the
@@ -404,11 +514,13 @@ int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out)
                          cudaGetErrorString(e));
     }
     if (cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->snap_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->retired_ev, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         if (s->adm) cudaStreamDestroy(s->adm);
+        if (s->snap_stream) cudaStreamDestroy(s->snap_stream);
         delete s;
-        return set_error(ctx, LGF_ECUDA, "cannot create the admission stream");
+        return set_error(ctx, LGF_ECUDA, "cannot create the admission streams");
     }
     for (int p = 0; p < 2; ++p) {
         s->shape[p] = serve_shape(ctx, p);  // jobs of every volume share the server's launches
@@ -417,6 +529,7 @@ int lgf_serve_start(lgf_ctx* ctx, const lgf_serve_config* cfg, lgf_server** out)
         const long long max_sites = (long long)(cfg->hbm_budget_bytes / per_site) + 1;
         s->max_tiles[p] = (4 * max_sites) / s->shape[p].threads + 2LL * cfg->max_active + 1;
     }
+    s->snap_thread = std::thread([s] { s->snap_run(); });
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return LGF_OK;
@@ -434,6 +547,7 @@ int lgf_serve_submit(lgf_server* s, const lgf_job* job, uint64_t* id) {
     j->job = *job;
     j->nmeas = nm;
     j->bytes = placed_bytes(job->shape, job->precision, nm);
+    if (job->snapshot_prefix) j->bytes += (snapshot_bytes(job->shape) + 255) & ~size_t(255);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) return LGF_ESHUTDOWN;
     if (j->bytes > s->cfg.hbm_budget_bytes) return LGF_ENOMEM;  // could never be admitted
@@ -500,6 +614,7 @@ int lgf_serve_stop(lgf_server* s) {
     }
     cudaEventDestroy(s->retired_ev);
     cudaStreamDestroy(s->adm);
+    cudaStreamDestroy(s->snap_stream);
     delete s;
     return LGF_OK;
 }

@@ -269,6 +269,7 @@ class Job:
     reunit_every: int = 0
     want_links: bool = False
     slices: bool = False
+    snapshot_prefix: str | None = None  # serving: links at each measurement -> <prefix>_Flowtime<t>.bin
     result: FlowResult | None = None
     links_out: np.ndarray | None = None
     _keep: list = field(default_factory=list, repr=False)
@@ -300,6 +301,10 @@ class Job:
                                  self.reunit_every)
         j.meas = ctypes.pointer(m)
         j.links_out = _dp(self.links_out)
+        if self.snapshot_prefix is not None:
+            pref = str(self.snapshot_prefix).encode()
+            self._keep.append(pref)
+            j.snapshot_prefix = pref
         return j
 
     def _collect(self):

@@ -113,3 +113,39 @@ def test_server_stop_while_threads_wait(ctx):
         assert not t.is_alive()
     for jid in ids:
         assert results[jid] == (C.LGF_OK, C.LGF_JOB_FAILED, C.LGF_ESHUTDOWN)
+
+
+def test_server_snapshots_at_measurements_and_resume(ctx, tmp_path):
+    """A served job with a snapshot prefix writes its links after every
+    measured step in the reference's flowed-file layout and naming; each file
+    equals the links lgf_flow reaches after that many steps, and a job resumed
+    from a snapshot (links = file, t0 = its flow time) ends on the same links
+    and E, Q as the uninterrupted job."""
+    U = golden_links("hb8_seed1.bin")
+    shape = (8, 8, 8, 8)
+    prefix = str(tmp_path / "torus_extdof4_0")
+    job = Job(shape, FP64, links=U, nsteps=30, meas_every=10, want_links=True, snapshot_prefix=prefix)
+    with Server(ctx, 1 << 30, max_active=2, steps_per_tick=4) as srv:
+        st = srv.wait(srv.submit(job), 120.0)
+    assert st.state == C.LGF_JOB_DONE and st.error == 0
+    for k, t in ((1, "0.100000"), (2, "0.200000"), (3, "0.300000")):
+        f = tmp_path / f"torus_extdof4_0_Flowtime{t}.bin"
+        _, ref = alone(ctx, Job(shape, FP64, links=U, nsteps=10 * k, meas_every=10))
+        assert np.array_equal(np.fromfile(f), ref), t
+    assert not (tmp_path / "torus_extdof4_0_Flowtime0.000000.bin").exists()  # the input itself is not written
+    snap = np.fromfile(tmp_path / "torus_extdof4_0_Flowtime0.200000.bin")
+    resumed = Job(shape, FP64, links=snap, t0=0.2, nsteps=10, meas_every=10, measure_at_t0=False, want_links=True)
+    with Server(ctx, 1 << 30, max_active=2) as srv:
+        st = srv.wait(srv.submit(resumed), 120.0)
+    assert st.state == C.LGF_JOB_DONE
+    assert np.array_equal(resumed.links_out, np.fromfile(tmp_path / "torus_extdof4_0_Flowtime0.300000.bin"))
+    assert abs(resumed.result.t[-1] - job.result.t[-1]) < 1e-12
+    assert resumed.result.E[-1] == job.result.E[-1] and resumed.result.Q[-1] == job.result.Q[-1]
+
+
+def test_server_snapshot_write_failure_fails_the_job(ctx, tmp_path):
+    job = Job((4, 4, 6, 6), FP64, seed=7, nsteps=4, meas_every=2,
+              snapshot_prefix=str(tmp_path / "no_such_dir" / "cfg"))
+    with Server(ctx, 1 << 28, max_active=1) as srv:
+        st = srv.wait(srv.submit(job), 60.0)
+    assert st.state == C.LGF_JOB_FAILED and st.error == C.LGF_EIO
