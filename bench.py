@@ -323,7 +323,8 @@ def form_batched(ctx):
                 seq += sec
         out[name] = {"site_steps_per_s": st.site_steps / st.seconds, "seconds": st.seconds,
                      "sequential_seconds": seq, "batching_speedup": seq / st.seconds,
-                     "launches": st.launches, "block_threads": st.block_threads}
+                     "launches": st.launches, "block_threads": st.block_threads,
+                     "tiles": ctx.get_tiles(prec, ENSEMBLE[-1][0])}
         results[name] = js
     dq = max(float(np.max(np.abs(a.result.Q - b.result.Q))) for a, b in zip(results["fp32mixed"], results["fp64"]))
     de = max(float(np.max(np.abs(a.result.E - b.result.E) / np.abs(b.result.E)))

@@ -82,12 +82,10 @@ int fetch_results(lgf_ctx* ctx, JobRun& r) {
     return LGF_OK;
 }
 
-// Flow one group of jobs (same precision) in lockstep; returns kernel launches.
-int run_group(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, const TileShape& shape, int* launches) {
-    long long tiles = 0;
-    for (auto* r : runs) tiles += (4LL * r->buf.g.V + shape.threads - 1) / shape.threads;
-    std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shape, (int)runs.size(), std::max(tiles, 1LL), true));
-    if (!grp) return ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
+// Flow one wave of jobs (same precision) in lockstep on the precision's group
+// (dynamic: the wave becomes its member set and the captured graphs stay
+// valid); adds the kernel launches issued to *launches.
+int run_wave(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, GroupBase* grp, int* launches) {
     std::vector<LatticeBuf*> members;
     std::vector<double> eps;
     for (auto* r : runs) {
@@ -243,8 +241,25 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
     for (int prec = 0; prec < 2 && rc == LGF_OK; ++prec) {
         if (groups[prec].empty()) continue;
         threads_used = shapes[prec].threads;
-        for (auto& wave : l2_waves(groups[prec], prec)) {
-            rc = run_group(ctx, prec, wave, shapes[prec], &launches);
+        // one group for every wave of this precision, sized for the largest:
+        // a wave replaces the previous one's members without a new group, a
+        // new capture or a device synchronisation in between
+        const auto waves = l2_waves(groups[prec], prec);
+        long long max_tiles = 1;
+        int max_members = 1;
+        for (const auto& wave : waves) {
+            long long t = 0;
+            for (auto* r : wave) t += (4LL * r->buf.g.V + shapes[prec].threads - 1) / shapes[prec].threads;
+            max_tiles = std::max(max_tiles, t);
+            max_members = std::max(max_members, (int)wave.size());
+        }
+        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shapes[prec], max_members, max_tiles, true));
+        if (!grp) {
+            rc = ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
+            break;
+        }
+        for (auto wave : waves) {
+            rc = run_wave(ctx, prec, wave, grp.get(), &launches);
             if (rc != LGF_OK) break;
         }
     }

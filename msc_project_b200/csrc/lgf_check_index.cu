@@ -8,8 +8,8 @@
 //   - the staple's neighbour sites x+mu, x+nu, x-nu, x-nu+mu (k_rk3_stage);
 //   - the loop walks of the measurement (Plane::advance) for every plane,
 //     quadrant and length 1..3;
-//   - the device layout (link_offset, alg_offset) is a bijection into the
-//     padded buffers;
+//   - the device layouts of both precisions (link_offset, alg_offset) are
+//     bijections into the padded buffers with 16-byte aligned vector loads;
 //   - the stage and measurement tile lists cover every tile exactly once for
 //     row-block and column orders and a range of budgets and block sizes.
 // Prints one line and exits 0 when everything holds.
@@ -103,20 +103,32 @@ static void check_plane_walks(const Geom& g) {
             }
 }
 
-static void check_layout(const Geom& g) {
+// the device layout of precision R is a bijection into the padded buffers,
+// and every vector load starts on a 16-byte boundary
+template <typename R> static void check_layout(const Geom& g) {
     const size_t Vp = padded_sites(g.V);
     std::vector<char> seen(Vp * 36, 0), seen_a(Vp * 32, 0);
     for (int s = 0; s < g.V; ++s)
         for (int mu = 0; mu < 4; ++mu) {
             for (int k = 0; k < 9; ++k) {
-                const size_t o = link_offset(mu, k, s);
+                const size_t o = link_offset<R>(mu, k, s);
                 CHECK(o < Vp * 36);
                 if (o < Vp * 36) CHECK(!seen[o]++);
             }
+            // double: every entry is a 16-byte load; float: entries 0, 2, 4, 6 start float4 loads
+            for (int k = 0; k < 9; ++k)
+                if (sizeof(R) == 8 || (k < 8 && k % 2 == 0)) CHECK((link_offset<R>(mu, k, s) * 2 * sizeof(R)) % 16 == 0);
+            if (sizeof(R) == 4)
+                for (int k = 0; k < 8; k += 2) CHECK(link_offset<R>(mu, k + 1, s) == link_offset<R>(mu, k, s) + 1);
             for (int a = 0; a < 8; ++a) {
-                const size_t o = alg_offset(mu, a, s);
+                const size_t o = alg_offset<R>(mu, a, s);
                 CHECK(o < Vp * 32);
                 if (o < Vp * 32) CHECK(!seen_a[o]++);
+            }
+            const int per = 16 / sizeof(R);  // reals of one vector load
+            for (int a = 0; a < 8; a += per) {
+                CHECK((alg_offset<R>(mu, a, s) * sizeof(R)) % 16 == 0);
+                for (int b = 1; b < per; ++b) CHECK(alg_offset<R>(mu, a + b, s) == alg_offset<R>(mu, a, s) + b);
             }
         }
 }
@@ -165,7 +177,8 @@ int main() {
         const Geom g = make_geom(sh);
         check_neighbours(g);
         check_plane_walks(g);
-        check_layout(g);
+        check_layout<double>(g);
+        check_layout<float>(g);
         check_tiles(g);
         ++n;
     }

@@ -58,12 +58,14 @@ size_t footprint_bytes(const int shape[4], int precision, int meas_slots) {
 // L1; 9% faster per stage than 128 on 24^3x48, 19% per job on 48^4), FP32 128
 // (three blocks per SM; 256 is 20% slower).
 #ifndef LGF_FP64_THREADS
-#define LGF_FP64_THREADS 256
+#define LGF_FP64_THREADS 384
 #endif
 #ifndef LGF_FP32_THREADS
 #define LGF_FP32_THREADS 128
 #endif
 int default_threads(int precision) { return precision == LGF_PREC_FP64 ? LGF_FP64_THREADS : LGF_FP32_THREADS; }
+
+int stage_max_threads(int precision) { return precision == LGF_PREC_FP64 ? LGF_STAGE_MAXT_D : LGF_STAGE_MAXT_F; }
 
 TileShape default_shape(int precision) {
     TileShape t;
@@ -234,50 +236,6 @@ __global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ 
     }
 }
 
-// ---------------------------------------------------------- pinned staging
-// Page-locked areas for the host->device copies of a group's lists.  A copy
-// from pageable memory may make the driver wait for the stream; from these
-// areas it never does.  Two areas are used in turn, and one is rewritten only
-// after the copies that last read it have completed (its event) -- normally
-// long before, since the other area was used in between.
-class PinnedStage {
-public:
-    ~PinnedStage() {
-        for (int k = 0; k < 2; ++k) {
-            if (ev_[k]) cudaEventSynchronize(ev_[k]);
-            if (ev_[k]) cudaEventDestroy(ev_[k]);
-            if (buf_[k]) cudaFreeHost(buf_[k]);
-        }
-    }
-    // an area of at least n bytes for the next copies
-    cudaError_t acquire(size_t n, char** out) {
-        cur_ ^= 1;
-        cudaError_t e = cudaSuccess;
-        if (!ev_[cur_]) e = cudaEventCreateWithFlags(&ev_[cur_], cudaEventDisableTiming);
-        else e = cudaEventSynchronize(ev_[cur_]);
-        if (e != cudaSuccess) return e;
-        if (cap_[cur_] < n) {
-            if (buf_[cur_]) cudaFreeHost(buf_[cur_]);
-            buf_[cur_] = nullptr;
-            cap_[cur_] = 0;
-            const size_t c = std::max<size_t>(n + n / 2, 4096);
-            e = cudaMallocHost(&buf_[cur_], c);
-            if (e != cudaSuccess) return e;
-            cap_[cur_] = c;
-        }
-        *out = buf_[cur_];
-        return cudaSuccess;
-    }
-    // the copies from the current area have been issued on stream s
-    cudaError_t release(cudaStream_t s) { return cudaEventRecord(ev_[cur_], s); }
-
-private:
-    char* buf_[2] = {nullptr, nullptr};
-    size_t cap_[2] = {0, 0};
-    cudaEvent_t ev_[2] = {nullptr, nullptr};
-    int cur_ = 1;
-};
-
 static inline size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
 
 // ------------------------------------------------------------------ groups
@@ -287,7 +245,7 @@ public:
         : ctx_(ctx), shape_(shape), threads_(shape.threads), max_members_(max_members), max_tiles_(max_tiles),
           dynamic_(dynamic) {}
     ~Group() override {
-        cudaStreamSynchronize(ctx_->stream);  // the lists and the staging areas are in use until then
+        cudaStreamSynchronize(ctx_->stream);  // the lists are in use until then
         if (step_exec_) cudaGraphExecDestroy(step_exec_);
         if (meas_exec_) cudaGraphExecDestroy(meas_exec_);
         cudaFree(d_desc_);
@@ -395,8 +353,9 @@ public:
         // one page-locked area carries the descriptors, both tile lists and the count
         const size_t bd = align16(sizeof(LatDesc<R>) * members.size()), bt = align16(sizeof(int2) * tiles.size()),
                      bm = align16(sizeof(int4) * mtiles.size());
+        std::lock_guard<std::mutex> lk(ctx_->list_mu);
         char* h = nullptr;
-        LGF_CUDA_TRY(ctx_, stage_.acquire(bd + bt + bm + 16, &h));
+        LGF_CUDA_TRY(ctx_, ctx_->list_stage.acquire(bd + bt + bm + 16, &h));
         std::memcpy(h, h_desc_.data(), sizeof(LatDesc<R>) * members.size());
         std::memcpy(h + bd, tiles.data(), sizeof(int2) * tiles.size());
         std::memcpy(h + bd + bt, mtiles.data(), sizeof(int4) * mtiles.size());
@@ -411,19 +370,20 @@ public:
             LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_all_mtiles_, h + bd + bt, sizeof(int4) * mtiles.size(),
                                                cudaMemcpyHostToDevice, ctx_->stream));
         LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_counts_, h + bd + bt + bm, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
-        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
+        LGF_CUDA_TRY(ctx_, ctx_->list_stage.release(ctx_->stream));
         return LGF_OK;
     }
 
     int set_eps(const std::vector<double>& eps) override {
         for (size_t i = 0; i < h_desc_.size() && i < eps.size(); ++i) h_desc_[i].eps = (R)eps[i];
         if (h_desc_.empty()) return LGF_OK;
+        std::lock_guard<std::mutex> lk(ctx_->list_mu);
         char* h = nullptr;
-        LGF_CUDA_TRY(ctx_, stage_.acquire(sizeof(LatDesc<R>) * h_desc_.size(), &h));
+        LGF_CUDA_TRY(ctx_, ctx_->list_stage.acquire(sizeof(LatDesc<R>) * h_desc_.size(), &h));
         std::memcpy(h, h_desc_.data(), sizeof(LatDesc<R>) * h_desc_.size());
         LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h, sizeof(LatDesc<R>) * h_desc_.size(), cudaMemcpyHostToDevice,
                                            ctx_->stream));
-        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
+        LGF_CUDA_TRY(ctx_, ctx_->list_stage.release(ctx_->stream));
         return LGF_OK;
     }
 
@@ -451,11 +411,14 @@ public:
         sel[0] = (int)which.size();
         sel[1] = (int)tm;
         sel[2] = (int)tr;
-        char* h = nullptr;
-        LGF_CUDA_TRY(ctx_, stage_.acquire(sizeof(int) * sel.size(), &h));
-        std::memcpy(h, sel.data(), sizeof(int) * sel.size());
-        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sel_, h, sizeof(int) * sel.size(), cudaMemcpyHostToDevice, ctx_->stream));
-        LGF_CUDA_TRY(ctx_, stage_.release(ctx_->stream));
+        {
+            std::lock_guard<std::mutex> lk(ctx_->list_mu);
+            char* h = nullptr;
+            LGF_CUDA_TRY(ctx_, ctx_->list_stage.acquire(sizeof(int) * sel.size(), &h));
+            std::memcpy(h, sel.data(), sizeof(int) * sel.size());
+            LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sel_, h, sizeof(int) * sel.size(), cudaMemcpyHostToDevice, ctx_->stream));
+            LGF_CUDA_TRY(ctx_, ctx_->list_stage.release(ctx_->stream));
+        }
         k_select_measure<<<dim3(std::max<int>(1, (int)which.size()), 16), 256, 0, ctx_->stream>>>(
             d_sel_, d_all_mtiles_, d_mtiles_, d_rtiles_, d_jobs_, d_counts_ + 1);
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
@@ -582,7 +545,6 @@ private:
     std::vector<LatticeBuf*> members_;
     std::vector<LatDesc<R>> h_desc_;
     std::vector<int> seg_off_, seg_len_;  // each member's segment of d_all_mtiles_
-    PinnedStage stage_;
     LatDesc<R>* d_desc_ = nullptr;
     int2* d_tiles_ = nullptr;
     int4* d_mtiles_ = nullptr;      // the measured members' tiles (k_select_measure)
@@ -600,7 +562,7 @@ private:
 
 GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
                       bool dynamic) {
-    if (shape.threads < 128 || shape.threads % 128 || shape.threads > LGF_STAGE_MAXT ||
+    if (shape.threads < 128 || shape.threads % 128 || shape.threads > stage_max_threads(precision) ||
         (shape.meas_split != 1 && shape.meas_split != 2) || shape.stage_budget <= 0 || shape.meas_budget <= 0) {
         set_error(ctx, LGF_EINVAL, "invalid tile shape (threads %d, measurement split %d)", shape.threads,
                   shape.meas_split);

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -34,7 +35,7 @@ namespace lgf {
 // for bit: only the block shapes and the order of the tiles change (no
 // reduction runs in tile order).
 struct TileShape {
-    int threads = 256;            // stage block size: a multiple of 128, at most LGF_STAGE_MAXT
+    int threads = 256;            // stage block size: a multiple of 128, at most stage_max_threads()
     int stage_order = 1;          // 0: blocks of x1 rows swept through x0; 1: x1 columns per CTA
     double stage_budget = 8.0 * (1 << 20);  // blocked order: stage bytes per row block and slice
     double meas_budget = 2.0 * (1 << 20);   // measurement: link bytes per row block and slice
@@ -45,6 +46,52 @@ struct TileShape {
     }
     bool operator!=(const TileShape& o) const { return !(*this == o); }
 };
+}  // namespace lgf
+
+namespace lgf {
+// Page-locked areas for the host->device copies of the groups' lists.  A copy
+// from pageable memory may make the driver wait for the stream; from these
+// areas it never does.  Two areas are used in turn, and one is rewritten only
+// after the copies that last read it have completed (its event) -- normally
+// long before, since the other area was used in between.
+class PinnedStage {
+public:
+    ~PinnedStage() {
+        for (int k = 0; k < 2; ++k) {
+            if (ev_[k]) cudaEventSynchronize(ev_[k]);
+            if (ev_[k]) cudaEventDestroy(ev_[k]);
+            if (buf_[k]) cudaFreeHost(buf_[k]);
+        }
+    }
+    // an area of at least n bytes for the next copies
+    cudaError_t acquire(size_t n, char** out) {
+        cur_ ^= 1;
+        cudaError_t e = cudaSuccess;
+        if (!ev_[cur_]) e = cudaEventCreateWithFlags(&ev_[cur_], cudaEventDisableTiming);
+        else e = cudaEventSynchronize(ev_[cur_]);
+        if (e != cudaSuccess) return e;
+        if (cap_[cur_] < n) {
+            if (buf_[cur_]) cudaFreeHost(buf_[cur_]);
+            buf_[cur_] = nullptr;
+            cap_[cur_] = 0;
+            const size_t c = std::max<size_t>(n + n / 2, 4096);
+            e = cudaMallocHost(&buf_[cur_], c);
+            if (e != cudaSuccess) return e;
+            cap_[cur_] = c;
+        }
+        *out = buf_[cur_];
+        return cudaSuccess;
+    }
+    // the copies from the current area have been issued on stream s
+    cudaError_t release(cudaStream_t s) { return cudaEventRecord(ev_[cur_], s); }
+
+private:
+    char* buf_[2] = {nullptr, nullptr};
+    size_t cap_[2] = {0, 0};
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    int cur_ = 1;
+};
+
 }  // namespace lgf
 
 struct lgf_ctx {
@@ -61,6 +108,11 @@ struct lgf_ctx {
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_done[2] = {nullptr, nullptr};
     std::mutex pin_mu;
+    // page-locked staging of the groups' list copies (shared by every group
+    // of the context, allocated on first use and kept: freeing page-locked
+    // memory would stall the device each time a group ends)
+    lgf::PinnedStage list_stage;
+    std::mutex list_mu;
 };
 
 namespace lgf {
@@ -77,6 +129,7 @@ int set_error(lgf_ctx* ctx, int code, const char* fmt, ...);
 bool valid_shape(const int shape[4]);
 size_t footprint_bytes(const int shape[4], int precision, int meas_slots);
 int default_threads(int precision);
+int stage_max_threads(int precision);  // the stage kernel's launch bound for this precision
 TileShape default_shape(int precision);
 // the tuned shape for a lattice of this precision and volume, else the default
 TileShape tuned_shape(const lgf_ctx* ctx, int precision, long long volume);

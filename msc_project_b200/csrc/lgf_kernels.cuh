@@ -24,10 +24,15 @@
 #pragma once
 #include "lgf_lattice.cuh"
 
-// Launch bounds of the two hot kernels: (max threads per block, min resident
-// blocks per SM).  The second number caps the registers per thread.
-#ifndef LGF_STAGE_MAXT
-#define LGF_STAGE_MAXT 256
+// Launch bounds of the RK3 stage: (max threads per block, min resident
+// blocks per SM), which cap the registers per thread.  double: up to 384
+// threads (12 warps per SM at 168 registers: 7% faster per stage than 8 warps
+// at 250 on 24^3x48 and 48^4); float: up to 256 (128-thread blocks, three per SM).
+#ifndef LGF_STAGE_MAXT_D
+#define LGF_STAGE_MAXT_D 384
+#endif
+#ifndef LGF_STAGE_MAXT_F
+#define LGF_STAGE_MAXT_F 256
 #endif
 #ifndef LGF_STAGE_MINB
 #define LGF_STAGE_MINB 1
@@ -73,88 +78,10 @@ __device__ __forceinline__ su3<R> staple_sum(const cplx<R>* __restrict__ U, cons
     return S;
 }
 
-// The same staple sum with each term built row by row from the left: row r
-// of U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag and of
-// U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu) as a row vector times two
-// matrices, so no 3x3 intermediate is held (the same 54 complex multiply-adds
-// per term; only the association differs, which changes rounding only).
-template <typename R>
-__device__ __forceinline__ su3<R> staple_sum_rows(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
-                                                  int mu) {
-    const int V = g.V;
-    const Dir dm = dir_of(g, c, mu);
-    su3<R> S;
-    su3_zero(S);
-    const int xpm = fwd(s, dm);
-#pragma unroll
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == mu) continue;
-        const int xpn = fwd(g, s, nu, c.x[nu]);
-        const int xmn = bwd(g, s, nu, c.x[nu]);
-        const int xmnpm = fwd(xmn, dm);
-        {
-            const su3<R> a3 = load_link(U, V, mu, xpn);
-            const su3<R> a2 = load_link(U, V, nu, s);
-            const cplx<R>* a1p = U + link_offset(nu, 0, xpm);
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                cplx<R> a1r[3], v[3];
-#pragma unroll
-                for (int j = 0; j < 3; ++j) a1r[j] = ldc(a1p + (3 * r + j) * LAYOUT_BLOCK);
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {  // v = a1[r,:] a3^dag
-                    cplx<R> t = cmulc(a1r[0], a3.m[3 * cc]);
-                    t = cfmac(a1r[1], a3.m[3 * cc + 1], t);
-                    v[cc] = cfmac(a1r[2], a3.m[3 * cc + 2], t);
-                }
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {  // S[r,:] += v a2^dag
-                    cplx<R> t = S.m[3 * r + cc];
-                    t = cfmac(v[0], a2.m[3 * cc], t);
-                    t = cfmac(v[1], a2.m[3 * cc + 1], t);
-                    S.m[3 * r + cc] = cfmac(v[2], a2.m[3 * cc + 2], t);
-                }
-            }
-        }
-        {
-            const su3<R> b1 = load_link(U, V, mu, xmn);
-            const su3<R> b3 = load_link(U, V, nu, xmn);
-            const cplx<R>* b2p = U + link_offset(nu, 0, xmnpm);
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                cplx<R> u[3], v[3];
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {  // row r of b2^dag: conj of column r of b2
-                    const cplx<R> z = ldc(b2p + (3 * j + r) * LAYOUT_BLOCK);
-                    u[j] = cmk<R>(z.re, -z.im);
-                }
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {  // v = u b1^dag
-                    cplx<R> t = cmulc(u[0], b1.m[3 * cc]);
-                    t = cfmac(u[1], b1.m[3 * cc + 1], t);
-                    v[cc] = cfmac(u[2], b1.m[3 * cc + 2], t);
-                }
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {  // S[r,:] += v b3
-                    cplx<R> t = S.m[3 * r + cc];
-                    t = cfma(v[0], b3.m[cc], t);
-                    t = cfma(v[1], b3.m[3 + cc], t);
-                    S.m[3 * r + cc] = cfma(v[2], b3.m[6 + cc], t);
-                }
-            }
-        }
-    }
-    return S;
-}
-
-#ifndef LGF_STAPLE_ROWS
-#define LGF_STAPLE_ROWS 0  // 1: build the staple terms row by row (staple_sum_rows)
-#endif
-
 template <typename R>
 __device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                 int mu, su3<R>& u_out) {
-    const su3<R> S = LGF_STAPLE_ROWS ? staple_sum_rows<R>(U, g, s, c, mu) : staple_sum<R>(U, g, s, c, mu);
+    const su3<R> S = staple_sum<R>(U, g, s, c, mu);
     u_out = load_link(U, g.V, mu, s);
     const su3<R> W = mul_nn(u_out, S);
     return ta_part(W, R(-0.5));
@@ -188,8 +115,11 @@ template <typename R> struct LatDesc {
 // all four directions: warp w handles mu = w % 4 for the 32 sites of group
 // w / 4, so the four link directions of a site range are read together and
 // every load of a warp covers 32 consecutive sites.
+template <typename R> struct StageMaxThreads { static constexpr int value = LGF_STAGE_MAXT_F; };
+template <> struct StageMaxThreads<double> { static constexpr int value = LGF_STAGE_MAXT_D; };
+
 template <typename R, int S>
-__global__ void __launch_bounds__(LGF_STAGE_MAXT, LGF_STAGE_MINB) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
+__global__ void __launch_bounds__(StageMaxThreads<R>::value, LGF_STAGE_MINB) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
                                                    const int* __restrict__ ntiles) {
     const int n = *ntiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
@@ -531,7 +461,7 @@ __global__ void __launch_bounds__(MEAS_SITES * 6 * QS, MeasMinBlocks<QS>::value)
     MeasSmem<R, OUT>* sm = reinterpret_cast<MeasSmem<R, OUT>*>(smem_raw);
     const int lane = threadIdx.x, w = threadIdx.y, p = w % 6, part = w / 6;
     constexpr int NW = 6 * QS;  // warps of the block
-    const int qa = part * (4 / QS), qb = qa + 4 / QS;
+    const int qa = part * 2, qb = qa + 2;  // QS = 2: this warp's quadrant half
     const int n = *nmtiles;
     for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
         const int4 tile = mtiles[ti];
@@ -561,9 +491,26 @@ __global__ void __launch_bounds__(MEAS_SITES * 6 * QS, MeasMinBlocks<QS>::value)
             store_line(sm, sdir, 3, lane, acc);
         }
         __syncthreads();
-        // phase 1: this thread's plane and quadrants
+        // phase 1: this thread's plane and quadrants; with one warp per plane
+        // the two quadrant halves are still summed apart and then added, the
+        // order two warps per plane use, so both give the same bits
         alg<R> G, Fh;
-        if (valid) plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, qa, qb, G, Fh);
+        if (valid) {
+            if (QS == 1) {
+#pragma unroll 1
+                for (int h = 0; h < 2; ++h) {
+                    alg<R> G1, F1;
+                    plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, 2 * h, 2 * h + 2, G1, F1);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        G.v[k] = h ? G.v[k] + G1.v[k] : G1.v[k];
+                        Fh.v[k] = h ? Fh.v[k] + F1.v[k] : F1.v[k];
+                    }
+                }
+            } else {
+                plane_fields_smem<R, OUT>(U, g, s, c, c_plane_mu[p], c_plane_nu[p], sm, lane, qa, qb, G, Fh);
+            }
+        }
         if (QS == 2) {
             __syncthreads();  // every warp is done with the lines
             if (part == 1 && valid) {
@@ -737,12 +684,11 @@ __global__ void __launch_bounds__(CONV_THREADS) k_to_device(const double2* __res
     const double2* src = file + (size_t)s0 * 36;
     for (int i = threadIdx.x; i < ns * 36; i += CONV_THREADS) t[(i / 36) * CONV_PITCH + i % 36] = src[i];
     __syncthreads();
-    cplx<R>* dst = U + (size_t)b * 36 * LAYOUT_BLOCK;
     for (int j = threadIdx.x; j < 36 * LAYOUT_BLOCK; j += CONV_THREADS) {
         const int e = j / LAYOUT_BLOCK, site = j % LAYOUT_BLOCK;
         if (site < ns) {
             const double2 v = t[site * CONV_PITCH + e];
-            stc(dst + j, cmk<R>((R)v.x, (R)v.y));
+            stc(U + link_offset<R>(e / 9, e % 9, s0 + site), cmk<R>((R)v.x, (R)v.y));
         }
     }
 }
@@ -753,11 +699,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_to_file(const cplx<R>* __restr
     const int b = blockIdx.x;
     const int s0 = b * LAYOUT_BLOCK;
     const int ns = min(LAYOUT_BLOCK, V - s0);
-    const cplx<R>* src = U + (size_t)b * 36 * LAYOUT_BLOCK;
     for (int j = threadIdx.x; j < 36 * LAYOUT_BLOCK; j += CONV_THREADS) {
         const int e = j / LAYOUT_BLOCK, site = j % LAYOUT_BLOCK;
         if (site < ns) {
-            const cplx<R> z = ldc(src + j);
+            const cplx<R> z = ldc(U + link_offset<R>(e / 9, e % 9, s0 + site));
             t[site * CONV_PITCH + e] = make_double2((double)z.re, (double)z.im);
         }
     }

@@ -7,14 +7,18 @@
 // One GPU holds the whole lattice, so there is no halo exchange.
 //
 // Device layout: blocks of 32 consecutive sites, each block holding every
-// entry of its sites' four links (structure of arrays inside the block):
-//   links  cplx<R>  U[((s/32)*36 + mu*9 + k) * 32 + s%32]    k = 3*row + col
-//   su(3)  R        A[((s/32)*32 + mu*8 + c) * 32 + s%32]    8 coordinates (lgf_su3.cuh)
-// A warp of 32 consecutive sites still reads 32 consecutive complex entries
-// (512 B for double, 256 B for float) per load instruction, and the links of
-// a site range sit together (18 KB per block in double) instead of in 36
-// arrays of V entries each: a stencil over a large lattice touches a few
-// pages per neighbour instead of dozens.  Buffers hold padded_sites(V) sites.
+// entry of its sites' four links (structure of arrays inside the block, see
+// link_offset / alg_offset below for the exact placement):
+//   links  36 complex entries per site and block row: double as 9 entry planes
+//          per direction (a lane reads 16 B per entry), float as 4 planes of
+//          entry pairs (16 B per lane) plus one plane of the 9th entry
+//   su(3)  8 coordinates per link (lgf_su3.cuh), pairs (double) or quads
+//          (float) per lane
+// Every load of a warp of 32 consecutive sites is one contiguous run (512 B),
+// and the links of a site range sit together (18 KB per block in double)
+// instead of in 36 arrays of V entries each: a stencil over a large lattice
+// touches a few pages per neighbour instead of dozens.  Buffers hold
+// padded_sites(V) sites.
 #pragma once
 #include <stdint.h>
 #include "lgf_su3.cuh"
@@ -133,40 +137,102 @@ template <typename R> __device__ __forceinline__ void stc(cplx<R>* p, cplx<R> z)
 #endif
 constexpr int LAYOUT_BLOCK = LGF_LAYOUT_BLOCK;  // sites per layout block
 __host__ __device__ __forceinline__ size_t padded_sites(size_t V) { return (V + LAYOUT_BLOCK - 1) / LAYOUT_BLOCK * LAYOUT_BLOCK; }
-// offset of complex entry k of link mu at site s; entry k+1 is LAYOUT_BLOCK further
-__host__ __device__ __forceinline__ size_t link_offset(int mu, int k, int s) {
+// Offset, in complex entries, of entry k (3*row + col) of link mu at site s.
+//   double: per 32-site block and direction, 9 entry planes of 32 sites: a
+//           lane's entry is one 16-byte double2 load, a warp's 512 B;
+//   float:  entries 0..7 in pairs -- plane p holds entries 2p and 2p+1 of each
+//           site side by side, one 16-byte float4 per lane -- and entry 8 in a
+//           plane of float2: a link is four 128-bit loads and one 64-bit load.
+// Both put the 36 entries of a block's four links in one contiguous run.
+template <typename R> __host__ __device__ __forceinline__ size_t link_offset(int mu, int k, int s) {
     LGF_INDEX_ASSERT(mu >= 0 && mu < 4 && k >= 0 && k < 9 && s >= 0);
-    return ((size_t)(s / LAYOUT_BLOCK) * 36 + mu * 9 + k) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
+    const size_t base = (size_t)(s / LAYOUT_BLOCK) * 36 * LAYOUT_BLOCK + (size_t)mu * 9 * LAYOUT_BLOCK;
+    const int l = s % LAYOUT_BLOCK;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        return base + (size_t)k * LAYOUT_BLOCK + l;
+    } else {
+        return k < 8 ? base + (size_t)(k >> 1) * 2 * LAYOUT_BLOCK + 2 * l + (k & 1) : base + 8 * LAYOUT_BLOCK + l;
+    }
 }
-__host__ __device__ __forceinline__ size_t alg_offset(int mu, int c, int s) {
+// Offset, in reals, of coordinate c of the su(3) accumulator of link mu at
+// site s: coordinates in pairs (double: one double2 per lane) or quads
+// (float: one float4 per lane), planes of 32 sites per block and direction.
+template <typename R> __host__ __device__ __forceinline__ size_t alg_offset(int mu, int c, int s) {
     LGF_INDEX_ASSERT(mu >= 0 && mu < 4 && c >= 0 && c < 8 && s >= 0);
-    return ((size_t)(s / LAYOUT_BLOCK) * 32 + mu * 8 + c) * LAYOUT_BLOCK + (s % LAYOUT_BLOCK);
+    const size_t base = (size_t)(s / LAYOUT_BLOCK) * 32 * LAYOUT_BLOCK + (size_t)mu * 8 * LAYOUT_BLOCK;
+    const int l = s % LAYOUT_BLOCK;
+    if constexpr (sizeof(R) == sizeof(double))
+        return base + (size_t)(c >> 1) * 2 * LAYOUT_BLOCK + 2 * l + (c & 1);
+    else
+        return base + (size_t)(c >> 2) * 4 * LAYOUT_BLOCK + 4 * l + (c & 3);
 }
 
 // (V is kept in the signatures: the lattice volume, no longer a stride)
 template <typename R> __device__ __forceinline__ su3<R> load_link(const cplx<R>* __restrict__ U, int V, int mu, int s) {
     su3<R> a;
-    const cplx<R>* p = U + link_offset(mu, 0, s);
+    if constexpr (sizeof(R) == sizeof(double)) {
+        const cplx<R>* p = U + link_offset<R>(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) a.m[k] = ldc(p + k * LAYOUT_BLOCK);
+        for (int k = 0; k < 9; ++k) a.m[k] = ldc(p + k * LAYOUT_BLOCK);
+    } else {
+        const float4* p = reinterpret_cast<const float4*>(U + link_offset<R>(mu, 0, s));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float4 v = __ldg(p + q * LAYOUT_BLOCK);
+            a.m[2 * q] = cmk<R>(v.x, v.y);
+            a.m[2 * q + 1] = cmk<R>(v.z, v.w);
+        }
+        a.m[8] = ldc(U + link_offset<R>(mu, 8, s));
+    }
     return a;
 }
 template <typename R> __device__ __forceinline__ void store_link(cplx<R>* __restrict__ U, int V, int mu, int s, const su3<R>& a) {
-    cplx<R>* p = U + link_offset(mu, 0, s);
+    if constexpr (sizeof(R) == sizeof(double)) {
+        cplx<R>* p = U + link_offset<R>(mu, 0, s);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) stc(p + k * LAYOUT_BLOCK, a.m[k]);
+        for (int k = 0; k < 9; ++k) stc(p + k * LAYOUT_BLOCK, a.m[k]);
+    } else {
+        float4* p = reinterpret_cast<float4*>(U + link_offset<R>(mu, 0, s));
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            p[q * LAYOUT_BLOCK] = make_float4(a.m[2 * q].re, a.m[2 * q].im, a.m[2 * q + 1].re, a.m[2 * q + 1].im);
+        stc(U + link_offset<R>(mu, 8, s), a.m[8]);
+    }
 }
 template <typename R> __device__ __forceinline__ alg<R> load_alg(const R* __restrict__ A, int V, int mu, int s) {
     alg<R> z;
-    const R* p = A + alg_offset(mu, 0, s);
+    if constexpr (sizeof(R) == sizeof(double)) {
+        const double2* p = reinterpret_cast<const double2*>(A + alg_offset<R>(mu, 0, s));
 #pragma unroll
-    for (int k = 0; k < 8; ++k) z.v[k] = __ldg(p + k * LAYOUT_BLOCK);
+        for (int q = 0; q < 4; ++q) {
+            const double2 v = __ldg(p + q * LAYOUT_BLOCK);
+            z.v[2 * q] = v.x;
+            z.v[2 * q + 1] = v.y;
+        }
+    } else {
+        const float4* p = reinterpret_cast<const float4*>(A + alg_offset<R>(mu, 0, s));
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float4 v = __ldg(p + q * LAYOUT_BLOCK);
+            z.v[4 * q] = v.x;
+            z.v[4 * q + 1] = v.y;
+            z.v[4 * q + 2] = v.z;
+            z.v[4 * q + 3] = v.w;
+        }
+    }
     return z;
 }
 template <typename R> __device__ __forceinline__ void store_alg(R* __restrict__ A, int V, int mu, int s, const alg<R>& z) {
-    R* p = A + alg_offset(mu, 0, s);
+    if constexpr (sizeof(R) == sizeof(double)) {
+        double2* p = reinterpret_cast<double2*>(A + alg_offset<R>(mu, 0, s));
 #pragma unroll
-    for (int k = 0; k < 8; ++k) p[k * LAYOUT_BLOCK] = z.v[k];
+        for (int q = 0; q < 4; ++q) p[q * LAYOUT_BLOCK] = make_double2(z.v[2 * q], z.v[2 * q + 1]);
+    } else {
+        float4* p = reinterpret_cast<float4*>(A + alg_offset<R>(mu, 0, s));
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            p[q * LAYOUT_BLOCK] = make_float4(z.v[4 * q], z.v[4 * q + 1], z.v[4 * q + 2], z.v[4 * q + 3]);
+    }
 }
 
 }  // namespace lgf

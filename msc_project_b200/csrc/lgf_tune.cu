@@ -4,7 +4,7 @@
 // On a lattice of the job's own shape (generated links; the volume decides
 // which orders keep the stencil's neighbours in L1/L2), candidates are timed
 // with CUDA events on the context's stream, one parameter at a time:
-//   stage:       block size {128, 256, 384 (if the launch bounds allow)},
+//   stage:       block size {128, 256, 384 (double only: the launch bounds)},
 //                then the tile order {x1 columns per CTA, row blocks through
 //                x0}, then (row blocks) the block budget {2, 8, 32 MB};
 //   measurement: warps per plane {2, 1}, then the block budget {2, 8, 64 MB}.
@@ -82,7 +82,7 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
         }
     };
     for (int th : {128, 256, 384}) {
-        if (th > LGF_STAGE_MAXT) continue;
+        if (th > stage_max_threads(prec)) continue;
         TileShape t = cur;
         t.threads = th;
         try_stage(t);
@@ -170,7 +170,8 @@ int lgf_set_tiles(lgf_ctx* ctx, int precision, const int shape[4], const lgf_til
     t.stage_budget = tiles->stage_budget_kb * 1024.0;
     t.meas_budget = tiles->meas_budget_kb * 1024.0;
     t.meas_split = tiles->meas_split;
-    if (t.threads < 128 || t.threads % 128 || t.threads > LGF_STAGE_MAXT || (t.stage_order != 0 && t.stage_order != 1) ||
+    if (t.threads < 128 || t.threads % 128 || t.threads > stage_max_threads(precision) ||
+        (t.stage_order != 0 && t.stage_order != 1) ||
         tiles->stage_budget_kb < 1 || tiles->meas_budget_kb < 1 || (t.meas_split != 1 && t.meas_split != 2))
         return set_error(ctx, LGF_EINVAL, "invalid tile shape");
     record_tuned(ctx, precision, 1LL * shape[0] * shape[1] * shape[2] * shape[3], t);
