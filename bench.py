@@ -382,11 +382,14 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
             ids.append(srv.submit(j))
         sts = [srv.wait(i, 3600.0) for i in ids]
         makespan = time.perf_counter() - t0
+        time.sleep(0.1)  # the scheduler counts the last ticks' device time
+        stats = srv.stats()
     lat = np.array([s.end_s - s.submit_s for s in sts])
     work = sum(int(np.prod(j.shape)) * j.nsteps for j in jobs)
     return {"jobs": njobs, "rate_per_s": rate if np.isfinite(rate) else "all at t=0", "jobs_per_s": njobs / makespan,
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "site_steps_per_s": work / makespan, "hbm_budget_bytes": budget,
+            "device_busy_frac": stats["device_busy_s"] / stats["wall_s"], "server_stats": stats,
             "all_done": all(s.state == 2 for s in sts)}
 
 
@@ -417,6 +420,9 @@ def engine_arm(args):
     prec = FP64 if args.precision == "fp64" else FP32MIXED
     V = int(np.prod(SHAPE))
     ctx = Context(local)
+    # tile shapes for this volume class, chosen once before any timing (the
+    # autotuner times its candidates on a lattice of this shape)
+    tiles = ctx.autotune_tiles(prec, SHAPE) if not args.no_autotune else ctx.get_tiles(prec, SHAPE)
     lat = ctx.lattice(SHAPE, prec)
     lat.generate(SEED, 0.5)
     reunit = 10 if prec == FP32MIXED else 0
@@ -517,6 +523,7 @@ def engine_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == FP64 else "f32+f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "precision": args.precision, "sites": V, "rk3_steps_per_step": NSTEPS,
+                   "tiles": tiles,
                    "measurements_per_step": nmeas, "l2": "inputs larger than L2 (382 MB links)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "site-RK3-steps/s", "h2d_bytes_per_step": V * 72 * 8,
@@ -560,13 +567,18 @@ def profile_case(args):
     import numpy as np
     from msc_project_b200 import FP32MIXED, FP64, Context
     prec = FP64 if args.precision == "fp64" else FP32MIXED
-    with Context(0) as ctx, ctx.lattice(SHAPE, prec) as lat:
+    with Context(0) as ctx:
+        if args.tiles:
+            ctx.set_tiles(prec, SHAPE, **json.loads(args.tiles))
+        lat = ctx.lattice(SHAPE, prec)
         lat.generate(SEED, 0.5)
         ms = (ctypes.c_double * 4)()
         ctx.check(ctx.lib.lgf_profile_kernels(lat.h, EPS, 1, ms))  # first launches load the modules
         ctx.check(ctx.lib.lgf_profile_kernels(lat.h, EPS, args.profile_reps, ms))
         print(json.dumps({"profile_case": list(SHAPE), "precision": args.precision,
-                          "stage_ms": [ms[0], ms[1], ms[2]], "measure_ms": ms[3]}))
+                          "tiles": ctx.get_tiles(prec, SHAPE), "stage_ms": [ms[0], ms[1], ms[2]],
+                          "measure_ms": ms[3]}))
+        lat.close()
 
 
 def main():
@@ -587,6 +599,8 @@ def main():
                     help="Poisson arrival rates (jobs/s) swept by the served form; inf = all jobs at t = 0")
     ap.add_argument("--profile", action="store_true", help="one launch of each kernel (for ncu captures)")
     ap.add_argument("--profile-reps", type=int, default=1)
+    ap.add_argument("--tiles", default="", help='--profile: tile shape fields as JSON, e.g. {"meas_budget_kb": 65536}')
+    ap.add_argument("--no-autotune", action="store_true", help="use the default tile shapes instead of tuning them")
     args = ap.parse_args()
     if args.profile:
         profile_case(args)

@@ -261,6 +261,22 @@ int lgf_serve_poll(lgf_server* srv, uint64_t id, lgf_job_status* st);
 int lgf_serve_wait(lgf_server* srv, uint64_t id, double timeout_s, lgf_job_status* st);
 int lgf_serve_stop(lgf_server* srv);
 
+/* Counters of a running server (no reference counterpart).  device_busy_s is
+ * the device time of the scheduling ticks, summed from CUDA events around each
+ * tick's launches (ticks whose events have not completed yet are left out);
+ * against the wall time since the start it shows how much of the stream the
+ * kernels themselves take. */
+typedef struct lgf_serve_stats {
+    double wall_s;             /* since lgf_serve_start */
+    double device_busy_s;      /* device time of completed ticks */
+    long long ticks;
+    long long steps;           /* RK3 steps launched (shared launches count once) */
+    long long measurements;    /* measurement launches (each covers the jobs due) */
+    long long jobs_done;
+    long long snapshots;
+} lgf_serve_stats;
+int lgf_serve_stats_get(lgf_server* srv, lgf_serve_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,12 @@ class lgf_serve_config(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int), ("steps_per_tick", ctypes.c_int)]
 
 
+class lgf_serve_stats(ctypes.Structure):
+    _fields_ = [("wall_s", ctypes.c_double), ("device_busy_s", ctypes.c_double), ("ticks", ctypes.c_longlong),
+                ("steps", ctypes.c_longlong), ("measurements", ctypes.c_longlong), ("jobs_done", ctypes.c_longlong),
+                ("snapshots", ctypes.c_longlong)]
+
+
 class lgf_job_status(ctypes.Structure):
     _fields_ = [("state", ctypes.c_int), ("error", ctypes.c_int), ("submit_s", ctypes.c_double),
                 ("start_s", ctypes.c_double), ("end_s", ctypes.c_double), ("steps_done", ctypes.c_int)]
@@ -104,6 +110,7 @@ SIGNATURES = {
     "lgf_serve_poll": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(lgf_job_status)]),
     "lgf_serve_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(lgf_job_status)]),
     "lgf_serve_stop": (ctypes.c_int, [_vp]),
+    "lgf_serve_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_serve_stats)]),
     "lgf_dropin_configure": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "lgf_dropin_flow_saved": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),

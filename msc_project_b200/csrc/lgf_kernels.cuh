@@ -25,14 +25,16 @@
 #include "lgf_lattice.cuh"
 
 // Launch bounds of the RK3 stage: (max threads per block, min resident
-// blocks per SM), which cap the registers per thread.  double: up to 384
-// threads (12 warps per SM at 168 registers: 7% faster per stage than 8 warps
-// at 250 on 24^3x48 and 48^4); float: up to 256 (128-thread blocks, three per SM).
+// blocks per SM), which cap the registers per thread at 65536 / 384 = 170,
+// i.e. 168 once rounded to the allocation unit.  double: 384-thread blocks
+// (12 warps per SM: 7% faster per stage than 8 warps at 250 registers on
+// 24^3x48 and 48^4); float: 128-thread blocks, three per SM (at 170
+// registers the rounding to 176 leaves room for only two: 15% slower).
 #ifndef LGF_STAGE_MAXT_D
 #define LGF_STAGE_MAXT_D 384
 #endif
 #ifndef LGF_STAGE_MAXT_F
-#define LGF_STAGE_MAXT_F 256
+#define LGF_STAGE_MAXT_F 384
 #endif
 #ifndef LGF_STAGE_MINB
 #define LGF_STAGE_MINB 1

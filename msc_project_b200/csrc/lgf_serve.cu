@@ -172,6 +172,14 @@ struct lgf_server {
     long long max_tiles[2] = {0, 0};
     int fatal = LGF_OK;
 
+    // statistics (worker thread; read under mu)
+    long long n_ticks = 0, n_steps = 0, n_meas = 0, n_done = 0, n_snap = 0;
+    double busy_s = 0.0;
+    struct TickEv { cudaEvent_t a, b; };
+    std::deque<TickEv> tick_ev;      // ticks whose device time is not counted yet
+    std::vector<TickEv> ev_free;     // recycled event pairs
+    void collect_ticks(bool wait);
+
     void run();
     void snap_run();
     int snapshot(ServeJob* j);
@@ -237,6 +245,10 @@ int lgf_server::snapshot(ServeJob* j) {
         cudaEventDestroy(t.ev);
         return set_error(ctx, LGF_ECUDA, "snapshot event failed: %s", cudaGetErrorString(e));
     }
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        ++n_snap;
+    }
     std::lock_guard<std::mutex> lk(snap_mu);
     j->snap_pending = true;
     snap_q.push_back(t);
@@ -260,6 +272,7 @@ void lgf_server::finish(ServeJob* j, int state, int err) {
     buf_free(j->buf);
     std::lock_guard<std::mutex> lk(mu);
     used -= j->bytes;
+    if (state == LGF_JOB_DONE) ++n_done;
     j->st.state = state;
     j->st.error = err;
     j->st.end_s = now_s(t0);
@@ -334,6 +347,10 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
                 if (e != LGF_OK) return e;
                 measured[p] = which;
             }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                ++n_meas;
+            }
             return group[p]->replay_measure();
         };
         // measurements at t0 for newly admitted jobs
@@ -367,6 +384,10 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
             }
             rc = group[p]->replay_step();
             if (rc != LGF_OK) return rc;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                ++n_steps;
+            }
             which.clear();
             for (size_t i = 0; i < run.size(); ++i) {
                 ServeJob* j = run[i];
@@ -396,9 +417,28 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
     return LGF_OK;
 }
 
+// add the device time of completed ticks to busy_s (all of them when wait)
+void lgf_server::collect_ticks(bool wait) {
+    while (!tick_ev.empty()) {
+        TickEv t = tick_ev.front();
+        if (wait) cudaEventSynchronize(t.b);
+        const cudaError_t q = cudaEventQuery(t.b);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) cudaGetLastError();
+        float ms = 0.f;
+        if (q == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            busy_s += ms * 1e-3;
+        }
+        tick_ev.pop_front();
+        ev_free.push_back(t);
+    }
+}
+
 void lgf_server::run() {
     cudaSetDevice(ctx->device);
     for (;;) {
+        collect_ticks(false);
         std::vector<ServeJob*> admitted;
         {
             std::unique_lock<std::mutex> lk(mu);
@@ -441,7 +481,25 @@ void lgf_server::run() {
         }
         staging.swap(still);
         if (active.empty()) continue;
+        TickEv te{nullptr, nullptr};
+        if (!ev_free.empty()) {
+            te = ev_free.back();
+            ev_free.pop_back();
+        } else if (cudaEventCreate(&te.a) != cudaSuccess || cudaEventCreate(&te.b) != cudaSuccess) {
+            cudaGetLastError();
+            te = {nullptr, nullptr};
+        }
+        if (te.a) cudaEventRecord(te.a, ctx->stream);
         int rc = tick(active);
+        if (te.a) {
+            cudaEventRecord(te.b, ctx->stream);
+            tick_ev.push_back(te);
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            ++n_ticks;
+        }
+        collect_ticks(false);
         if (rc != LGF_OK) {
             for (auto* j : active) finish(j, LGF_JOB_FAILED, rc);
             active.clear();
@@ -462,6 +520,12 @@ void lgf_server::run() {
     }
     cudaStreamSynchronize(ctx->stream);
     cudaStreamSynchronize(adm);
+    collect_ticks(true);
+    for (auto& t : ev_free) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    ev_free.clear();
     for (auto* j : staging) finish(j, LGF_JOB_FAILED, LGF_ESHUTDOWN);
     staging.clear();
     for (auto* j : active) finish(j, LGF_JOB_FAILED, LGF_ESHUTDOWN);
@@ -558,6 +622,19 @@ int lgf_serve_submit(lgf_server* s, const lgf_job* job, uint64_t* id) {
     s->queue.push_back(j.get());
     s->jobs[j->id] = std::move(j);
     s->cv_work.notify_all();
+    return LGF_OK;
+}
+
+int lgf_serve_stats_get(lgf_server* s, lgf_serve_stats* st) {
+    if (!s || !st) return LGF_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    st->wall_s = now_s(s->t0);
+    st->device_busy_s = s->busy_s;
+    st->ticks = s->n_ticks;
+    st->steps = s->n_steps;
+    st->measurements = s->n_meas;
+    st->jobs_done = s->n_done;
+    st->snapshots = s->n_snap;
     return LGF_OK;
 }
 

@@ -4,7 +4,7 @@
 // On a lattice of the job's own shape (generated links; the volume decides
 // which orders keep the stencil's neighbours in L1/L2), candidates are timed
 // with CUDA events on the context's stream, one parameter at a time:
-//   stage:       block size {128, 256, 384 (double only: the launch bounds)},
+//   stage:       block size {128, 256, 384},
 //                then the tile order {x1 columns per CTA, row blocks through
 //                x0}, then (row blocks) the block budget {2, 8, 32 MB};
 //   measurement: warps per plane {2, 1}, then the block budget {2, 8, 64 MB}.

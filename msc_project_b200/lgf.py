@@ -333,6 +333,12 @@ class Server:
         self._jobs[jid.value] = job
         return jid.value
 
+    def stats(self) -> dict:
+        """Counters of the running server (lgf_serve_stats_get)."""
+        st = C.lgf_serve_stats()
+        self.ctx.check(self.lib.lgf_serve_stats_get(self.h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in C.lgf_serve_stats._fields_}
+
     def poll(self, jid: int):
         st = C.lgf_job_status()
         rc = self.lib.lgf_serve_poll(self.h, ctypes.c_uint64(jid), ctypes.byref(st))

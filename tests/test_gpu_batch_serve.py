@@ -127,7 +127,12 @@ def test_server_snapshots_at_measurements_and_resume(ctx, tmp_path):
     job = Job(shape, FP64, links=U, nsteps=30, meas_every=10, want_links=True, snapshot_prefix=prefix)
     with Server(ctx, 1 << 30, max_active=2, steps_per_tick=4) as srv:
         st = srv.wait(srv.submit(job), 120.0)
+        time.sleep(0.2)
+        stats = srv.stats()
     assert st.state == C.LGF_JOB_DONE and st.error == 0
+    assert stats["snapshots"] == 3 and stats["jobs_done"] == 1 and stats["steps"] == 30
+    assert stats["measurements"] == 4 and stats["ticks"] >= 8
+    assert 0 < stats["device_busy_s"] <= stats["wall_s"]
     for k, t in ((1, "0.100000"), (2, "0.200000"), (3, "0.300000")):
         f = tmp_path / f"torus_extdof4_0_Flowtime{t}.bin"
         _, ref = alone(ctx, Job(shape, FP64, links=U, nsteps=10 * k, meas_every=10))
