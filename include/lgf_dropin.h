@@ -117,6 +117,13 @@ extern "C" {
 /* precision: LGF_PREC_FP64 (0) or LGF_PREC_FP32MIXED (1); reunit_every applies
  * to the mixed form (0 = never); device = CUDA device ordinal */
 int lgf_dropin_configure(int precision, int reunit_every, int device);
+/* FlowSavedGaugeConfigurations flows up to `configs` saved configurations
+ * together through lgf_batch_run (1 = one by one, the default; the
+ * environment variable LGF_BATCH sets it too) and writes the same stdout
+ * lines, CSV rows and flowed files, in the same order, with the same values
+ * bit for bit.  No reference counterpart (the reference flows one at a time,
+ * LGF/LGF.cpp:169-195). */
+int lgf_dropin_set_batch(int configs);
 
 /* Flat C entry points with the reference's arguments (for cgo/ctypes/JNI).
  * Return 0 on success, a negative LGF_E* status when a configuration failed

@@ -112,6 +112,7 @@ SIGNATURES = {
     "lgf_serve_stop": (ctypes.c_int, [_vp]),
     "lgf_serve_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(lgf_serve_stats)]),
     "lgf_dropin_configure": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "lgf_dropin_set_batch": (ctypes.c_int, [ctypes.c_int]),
     "lgf_dropin_flow_saved": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_char_p]),
     "lgf_dropin_resume_flowed": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <filesystem>
 #include <fstream>
 #include <iostream>
@@ -32,6 +33,7 @@ struct DropinState {
     int precision = -1;
     int reunit_every = 10;
     int device = -1;
+    int batch = -1;  // configurations flowed together by FlowSavedGaugeConfigurations (1 = one by one)
 };
 DropinState g_state;
 
@@ -209,8 +211,105 @@ SimulationParameters::SimulationParameters(int NrDims, int extdofs, std::vector<
     }
 }
 
+static int env_batch() {
+    const char* b = std::getenv("LGF_BATCH");
+    return b ? std::max(1, std::atoi(b)) : 1;
+}
+
+// FlowSavedGaugeConfigurations with up to g_state.batch configurations flowed
+// together by lgf_batch_run (shared launches, one graph per RK3 step); each
+// configuration's stdout lines, CSV rows and flowed file follow in the
+// reference's order once its chunk is done.  The results are the same bits as
+// flowing them one by one.
+static int flow_saved_batched(SimulationParameters& params, FlowParameters& fp, lgf_ctx* ctx) {
+    const std::string UpdateMethod = "LHMC_3_of_0_330000";  // LGF.cpp:164
+    const long long V = 1LL * params.getshape(0) * params.getshape(1) * params.getshape(2) * params.getshape(3);
+    const int shape[4] = {params.getshape(0), params.getshape(1), params.getshape(2), params.getshape(3)};
+    const int steps = fp.getflowSteps(), meas = fp.getMeasuringInterval();
+    const int nm = 1 + (meas > 0 ? steps / meas : 0);
+    double flowTime = 0.0;
+    for (int s = 0; s < steps; ++s) flowTime += fp.getepsilon();  // GradientFlow.cpp:52
+    int status = LGF_OK;
+    for (int c0 = fp.getConfigurationStart(); c0 <= fp.getConfigurationStop(); c0 += g_state.batch) {
+        const int c1 = std::min(fp.getConfigurationStop(), c0 + g_state.batch - 1);
+        struct Cfg {
+            int id;
+            std::vector<double> links, t, E, Q;
+            lgf_meas m;
+        };
+        std::vector<Cfg> cfgs;
+        cfgs.reserve(c1 - c0 + 1);
+        for (int i = c0; i <= c1; ++i) {
+            Cfg c;
+            c.id = i;
+            c.links.resize((size_t)V * 4 * 18);
+            if (!load_links(params, UpdateMethod, fp.getdataFolder(), std::to_string(i), c.links)) {
+                status = LGF_EIO;
+                continue;
+            }
+            c.t.assign(nm, 0.0);
+            c.E.assign(nm, 0.0);
+            c.Q.assign(nm, 0.0);
+            cfgs.push_back(std::move(c));
+        }
+        if (cfgs.empty()) continue;
+        std::vector<lgf_job> jobs(cfgs.size());
+        for (size_t k = 0; k < cfgs.size(); ++k) {
+            Cfg& c = cfgs[k];
+            c.m = lgf_meas{};
+            c.m.capacity = nm;
+            c.m.t = c.t.data();
+            c.m.E = c.E.data();
+            c.m.Q = c.Q.data();
+            lgf_job& j = jobs[k];
+            j = lgf_job{};
+            std::memcpy(j.shape, shape, sizeof shape);
+            j.precision = g_state.precision;
+            j.links = c.links.data();
+            j.flow.eps = fp.getepsilon();
+            j.flow.nsteps = steps;
+            j.flow.meas_every = meas;
+            j.flow.t0 = 0.0;
+            j.flow.measure_at_t0 = 1;
+            j.flow.reunit_every = g_state.precision == LGF_PREC_FP32MIXED ? g_state.reunit_every : 0;
+            j.meas = &c.m;
+            j.links_out = c.links.data();  // read at admission, written at the end
+        }
+        const int rc = lgf_batch_run(ctx, jobs.data(), (int)jobs.size(), nullptr);
+        if (rc != LGF_OK) {
+            std::cout << "LGF engine: " << lgf_last_error(ctx) << "\n";
+            status = rc;
+            continue;
+        }
+        for (Cfg& c : cfgs) {
+            for (int i = 0; i < nm; ++i) {
+                std::cout << "Topological Charge = " << c.Q[i] << "\n";
+                std::cout.flush();
+                std::cout << "Energy Density\t   = " << c.E[i] << "\n";
+                std::cout.flush();
+            }
+            const std::string ensembleNum = std::to_string(c.id);
+            append_csv(params, "Topological_Charge", "GF", fp.getdataFolder(), "_" + ensembleNum, c.t, c.Q);
+            append_csv(params, "EnergyDensity", "GF", fp.getdataFolder(), "_" + ensembleNum, c.t, c.E);
+            if (!save_links(params, "GF", fp.getdataFolder(), ensembleNum + "_Flowtime" + std::to_string(flowTime),
+                            c.links))
+                status = LGF_EIO;
+        }
+    }
+    return status;
+}
+
 static int flow_saved_impl(SimulationParameters& params, FlowParameters& fp) {
     if (!check_params(params)) return LGF_EINVAL;
+    if (g_state.batch < 0) g_state.batch = env_batch();
+    if (g_state.batch > 1) {
+        int rc = LGF_OK;
+        lgf_ctx* ctx = context(&rc);
+        if (!ctx) return rc;
+        const long long V = 1LL * params.getshape(0) * params.getshape(1) * params.getshape(2) * params.getshape(3);
+        std::cout << "total Volume: " << V << std::endl;  // Lattice.cpp:199
+        return flow_saved_batched(params, fp, ctx);
+    }
     int rc = LGF_OK;
     lgf_ctx* ctx = nullptr;
     const std::string UpdateMethod = "LHMC_3_of_0_330000";  // LGF.cpp:164
@@ -448,6 +547,12 @@ int lgf_dropin_configure(int precision, int reunit_every, int device) {
     g_state.precision = precision;
     g_state.reunit_every = reunit_every;
     g_state.device = device;
+    return LGF_OK;
+}
+
+int lgf_dropin_set_batch(int configs) {
+    if (configs < 1) return LGF_EINVAL;
+    g_state.batch = configs;
     return LGF_OK;
 }
 

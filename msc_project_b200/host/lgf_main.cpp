@@ -4,7 +4,7 @@
 //   lgf_flow NrDims extdofs beta shape[NrDims] cuts[NrDims] configStart configStop
 //            flowSteps epsilon measureInterval dataFolder
 //            [--workflow flow|resume=<t>|qdensity|measure] [--precision fp64|fp32mixed]
-//            [--reunit-every k] [--device d]
+//            [--reunit-every k] [--device d] [--batch n]
 //
 // cuts are accepted and ignored (one GPU holds the whole lattice).  The
 // workflow defaults to FlowSavedGaugeConfigurations; an integer in the epsilon
@@ -23,7 +23,7 @@
 int main(int argc, char** argv) {
     std::vector<std::string> pos;
     std::string workflow = "flow";
-    int precision = LGF_PREC_FP64, reunit = 10, device = 0;
+    int precision = LGF_PREC_FP64, reunit = 10, device = 0, batch = 0;
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
         if (a.rfind("--workflow=", 0) == 0) workflow = a.substr(11);
@@ -32,6 +32,7 @@ int main(int argc, char** argv) {
         else if (a == "--precision" && i + 1 < argc) precision = std::string(argv[++i]) == "fp32mixed" ? LGF_PREC_FP32MIXED : LGF_PREC_FP64;
         else if (a == "--reunit-every" && i + 1 < argc) reunit = std::atoi(argv[++i]);
         else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
+        else if (a == "--batch" && i + 1 < argc) batch = std::atoi(argv[++i]);
         else pos.push_back(a);
     }
     if (pos.size() < 3) {
@@ -65,7 +66,8 @@ int main(int argc, char** argv) {
     const std::string folder = pos[i++];
     if (heatbath && workflow == "flow") workflow = "heatbath";
     std::cout << "Started Parallel Session with 1 processes...\n";
-    if (lgf_dropin_configure(precision, reunit, device) != LGF_OK) {
+    if (lgf_dropin_configure(precision, reunit, device) != LGF_OK ||
+        (batch > 0 && lgf_dropin_set_batch(batch) != LGF_OK)) {
         std::cerr << "lgf_flow: bad engine options\n";
         return 2;
     }

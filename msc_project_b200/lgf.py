@@ -382,9 +382,13 @@ class FlowParameters:
         self.epsilon, self.measureEvery, self.dataFolder = epsilon, measure_every_nth_step, dataFolder
 
 
-def configure(precision=FP64, reunit_every: int = 10, device: int = 0):
+def configure(precision=FP64, reunit_every: int = 10, device: int = 0, batch: int = 1):
+    """Engine options of the drop-in workflows; batch > 1 flows that many saved
+    configurations together in FlowSavedGaugeConfigurations."""
     lib = C.load()
     rc = lib.lgf_dropin_configure(precision_code(precision), reunit_every, device)
+    if rc == C.LGF_OK:
+        rc = lib.lgf_dropin_set_batch(batch)
     if rc != C.LGF_OK:
         raise LGFError(rc, "bad drop-in configuration")
 

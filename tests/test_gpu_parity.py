@@ -460,3 +460,31 @@ def test_long_flow_against_oracle(ctx):
     assert rel_err(r.E, E) < 1e-12 and q_err(r.Q, Q) < 1e-12
     assert np.max(np.abs(Ug - Uo)) < 1e-12
     assert u < 1e-13 and d < 1e-13
+
+
+def test_dropin_batched_equals_one_by_one(ctx, tmp_path):
+    """FlowSavedGaugeConfigurations with its configurations flowed together
+    (lgf_dropin_set_batch) writes the same CSV bytes and the same flowed files,
+    bit for bit, as flowing them one by one; a missing configuration is
+    skipped and reported in both modes."""
+    from msc_project_b200 import FlowParameters, FlowSavedGaugeConfigurations, SimulationParameters, configure
+    shape = [8, 8, 8, 8]
+    outs = {}
+    for batch in (1, 3):
+        root = tmp_path / f"b{batch}"
+        d = root / "ensembles/su3/beta6_000000/8X8X8X8/LHMC_3_of_0_330000"
+        d.mkdir(parents=True)
+        (d / "torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
+        O.generate_G(tuple(shape), 3, 0.5).tofile(d / "torus_extdof4_1.bin")
+        O.generate_G(tuple(shape), 4, 0.5).tofile(d / "torus_extdof4_3.bin")  # configuration 2 is missing
+        configure(FP64, batch=batch)
+        rc = FlowSavedGaugeConfigurations(SimulationParameters(4, 4, shape, 6.0, [0, 0, 0, 0]),
+                                          FlowParameters(0, 3, 20, 0.01, 5, str(root) + "/"))
+        files = {p.relative_to(root).as_posix(): p.read_bytes() for p in root.rglob("*")
+                 if p.is_file() and "LHMC" not in p.as_posix()}
+        outs[batch] = (rc, files)
+    configure(FP64)
+    assert outs[1][0] == outs[3][0] != 0  # the missing configuration is reported
+    assert set(outs[1][1]) == set(outs[3][1]) and len(outs[1][1]) == 3 * 3
+    for k, v in outs[1][1].items():
+        assert outs[3][1][k] == v, k
