@@ -194,7 +194,8 @@ def run_reference_sample(nproc: int, steps: int, warm: int, shape=REF_SAMPLE_SHA
     nmeas = 1 + NSTEPS // MEAS
     job_s = NSTEPS * t_step + nmeas * meas_s  # one process's job on the sample lattice
     value = nproc * V * NSTEPS / job_s
-    return {"value": value, "per_step_s": per_step, "measure_s": meas_s, "cores": nproc,
+    return {"value": value, "per_step_s": per_step, "measure_s": meas_s, "cores": nproc, "host_cpu": host_cpu(),
+            "host_threads": os.cpu_count(),
             "flow_only": nproc * V / t_step,
             "lattice_setup_s": max(r["setup_s"] for r in res),
             "sample": f"{nproc} parallel single-rank reference processes (no MPI on the host), each the "
@@ -202,6 +203,17 @@ def run_reference_sample(nproc: int, steps: int, warm: int, shape=REF_SAMPLE_SHA
                       f"one (first {warm} untimed) and one E/Q measurement; rate = the bench job's schedule "
                       f"({NSTEPS} steps + {nmeas} measurements) at the slowest process's median step and "
                       f"measurement times; the Lattice/field setup and input read (lattice_setup_s) is excluded"}, None
+
+
+def host_cpu() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the baseline record."""
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def _ref_shape(args):
@@ -228,7 +240,8 @@ def reference_arm(args):
                    "step": "one RK3 step of every process (wall, slowest process); one E/Q measurement after them"},
         "cpu_baseline": {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"],
                          "kind": "reference", "sample": res["sample"], "measure_s": res["measure_s"],
-                         "flow_only": res["flow_only"], "lattice_setup_s": res["lattice_setup_s"]},
+                         "flow_only": res["flow_only"], "lattice_setup_s": res["lattice_setup_s"],
+                         "host_cpu": res["host_cpu"], "host_threads": res["host_threads"]},
         "e2e": {"value": res["value"], "unit": "site-RK3-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -497,7 +510,8 @@ def engine_arm(args):
         if res:
             cpu = {"value": res["value"], "unit": "site-RK3-steps/s", "cores": res["cores"], "kind": "reference",
                    "sample": res["sample"], "measure_s": res["measure_s"], "flow_only": res["flow_only"],
-                   "lattice_setup_s": res["lattice_setup_s"]}
+                   "lattice_setup_s": res["lattice_setup_s"], "host_cpu": res["host_cpu"],
+                   "host_threads": res["host_threads"]}
         else:
             cpu = {"value": None, "unavailable": err}
 

@@ -11,7 +11,8 @@
 //   - the device layouts of both precisions (link_offset, alg_offset) are
 //     bijections into the padded buffers with 16-byte aligned vector loads;
 //   - the stage and measurement tile lists cover every tile exactly once for
-//     row-block and column orders and a range of budgets and block sizes.
+//     row-block and column orders and a range of budgets and block sizes, and
+//     the measurement's strips or patches cover every site of a slice once.
 // Prints one line and exits 0 when everything holds.
 #include <cstdio>
 #include <cstdlib>
@@ -157,6 +158,17 @@ static void check_tiles(const Geom& g) {
         }
     }
     const int nchunk = (g.Vs + MEAS_SITES - 1) / MEAS_SITES;
+    // every site of a slice is exactly one lane of one chunk
+    {
+        std::vector<char> hit(g.Vs, 0);
+        for (int c = 0; c < nchunk; ++c)
+            for (int l = 0; l < MEAS_SITES; ++l) {
+                const int off = meas_site_offset(g, meas_patched(g), c, l);
+                if (off < g.Vs) CHECK(!hit[off]++);
+                else CHECK(!meas_patched(g));  // only a strip's last chunk runs past the slice
+            }
+        for (int o = 0; o < g.Vs; ++o) CHECK(hit[o] == 1);
+    }
     for (double budget : {1.0e3, 2.0e4, 3.0e5, 2.0e6, 6.4e7}) {
         std::vector<int4> tiles;
         append_measure_tiles(tiles, 2, g, budget, bps_meas);
@@ -171,7 +183,7 @@ static void check_tiles(const Geom& g) {
 
 int main() {
     const int shapes[][4] = {{4, 4, 4, 4}, {4, 6, 8, 10}, {6, 6, 6, 6}, {4, 4, 6, 6}, {8, 4, 6, 4},
-                             {10, 4, 4, 8}, {4, 20, 18, 18}, {4, 6, 6, 10}};
+                             {10, 4, 4, 8}, {4, 20, 18, 18}, {4, 6, 6, 10}, {4, 6, 8, 16}, {6, 4, 12, 8}};
     int n = 0;
     for (const auto& sh : shapes) {
         const Geom g = make_geom(sh);

@@ -296,6 +296,32 @@ __device__ __constant__ int c_plane_mu[6] = {0, 0, 0, 1, 1, 2};
 __device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
 
 constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
+
+// Measurement tile geometry.  A tile's 32 sites are a patch of 4 x2 rows by 8
+// x3 positions at fixed (x0, x1) when N2 % 4 == 0 and N3 % 8 == 0, else 32
+// consecutive sites of the slice (a strip).  The patch keeps the +-3 stencil of
+// the six planes compact: a strip along x3 touches ~5500 distinct sites per
+// tile, a 4 x 8 patch ~3600, and each warp load still covers four whole
+// 128-byte lines (8 consecutive sites per row).  Chunk c of a slice is patch
+// (x1, b2, b3) = (c / (nb2 nb3), (c / nb3) % nb2, c % nb3); a slice has
+// Vs / 32 chunks either way.  A fixed function of the lattice shape, so the
+// grouping of the partial sums (and every result bit) does not depend on tile
+// shapes or batch partners.
+#ifndef LGF_MEAS_PATCH
+#define LGF_MEAS_PATCH 1
+#endif
+constexpr int MEAS_PATCH_ROWS = 4, MEAS_PATCH_COLS = 8;
+__host__ __device__ __forceinline__ bool meas_patched(const Geom& g) {
+    return LGF_MEAS_PATCH && g.n[2] % MEAS_PATCH_ROWS == 0 && g.n[3] % MEAS_PATCH_COLS == 0;
+}
+// offset within its x0 slice of lane l's site in measurement chunk c
+__host__ __device__ __forceinline__ int meas_site_offset(const Geom& g, bool patched, int c, int l) {
+    if (!patched) return c * MEAS_SITES + l;
+    const int nb3 = g.n[3] / MEAS_PATCH_COLS, nb2 = g.n[2] / MEAS_PATCH_ROWS;
+    const int x1 = c / (nb2 * nb3), r = c - x1 * (nb2 * nb3), b2 = r / nb3, b3 = r - b2 * nb3;
+    return (x1 * g.n[2] + b2 * MEAS_PATCH_ROWS + l / MEAS_PATCH_COLS) * g.n[3] + b3 * MEAS_PATCH_COLS +
+           l % MEAS_PATCH_COLS;
+}
 constexpr int MEAS_QSPLIT = LGF_MEAS_QSPLIT;
 constexpr int MEAS_WARPS = 6 * MEAS_QSPLIT;  // warp y: plane y % 6, quadrants of part y / 6
 // resident measurement blocks per SM the launch bounds ask for (caps the
@@ -470,7 +496,7 @@ __global__ void __launch_bounds__(MEAS_SITES * 6 * QS, MeasMinBlocks<QS>::value)
         const LatDesc<R>* d = descs + tile.x;
         const Geom g = d->g;
         const int slice = tile.y, chunk = tile.z;
-        const int off = chunk * MEAS_SITES + lane;
+        const int off = meas_site_offset(g, meas_patched(g), chunk, lane);
         const bool valid = off < g.Vs;
         const int s = slice * g.Vs + (valid ? off : 0);
         const Coord c = site_coord(g, s);

@@ -36,7 +36,7 @@ struct SiteBlock { int a1, b1, a2, b2; };
 #endif
 constexpr int MIN_ROWS = LGF_MIN_ROWS;
 
-inline std::vector<SiteBlock> site_blocks(const Geom& g, double budget, double bytes_per_site) {
+inline std::vector<SiteBlock> site_blocks(const Geom& g, double budget, double bytes_per_site, int align2 = 1) {
     std::vector<SiteBlock> out;
     const int N1 = g.n[1], N2 = g.n[2], N3 = g.n[3];
     const double sites = budget / bytes_per_site;  // sites of one block and slice
@@ -46,7 +46,8 @@ inline std::vector<SiteBlock> site_blocks(const Geom& g, double budget, double b
         const int r = std::max(1, (int)(sites / ((double)N2 * N3)));
         for (int a = 0; a < N1; a += r) out.push_back({a, std::min(a + r, N1), 0, N2});
     } else {
-        const int side = std::max(1, (int)std::sqrt(sites / N3));
+        // square blocks; x2 boundaries on multiples of align2 (the measurement's patch rows)
+        const int side = std::max(align2, (int)std::sqrt(sites / N3) / align2 * align2);
         for (int a = 0; a < N1; a += side)
             for (int c = 0; c < N2; c += side) out.push_back({a, std::min(a + side, N1), c, std::min(c + side, N2)});
     }
@@ -89,10 +90,20 @@ inline bool append_stage_tiles_columns(std::vector<int2>& tiles, int i, const Ge
     return true;
 }
 
-// measurement tiles (lattice, slice, 32-site chunk of the slice) of lattice i
+// measurement tiles (lattice, slice, chunk of the slice) of lattice i; a
+// chunk is a 32-site strip or a 4 x 8 patch (meas_patched, lgf_kernels.cuh)
 inline void append_measure_tiles(std::vector<int4>& tiles, int i, const Geom& g, double budget,
                                  double bytes_per_site) {
     const long long N3 = g.n[3], row = (long long)g.n[2] * N3;
+    if (meas_patched(g)) {
+        const int nb3 = g.n[3] / MEAS_PATCH_COLS, nb2 = g.n[2] / MEAS_PATCH_ROWS;
+        for (const SiteBlock& b : site_blocks(g, budget, bytes_per_site, MEAS_PATCH_ROWS))
+            for (int t = 0; t < g.n[0]; ++t)
+                for (int x1 = b.a1; x1 < b.b1; ++x1)
+                    for (int c2 = b.a2 / MEAS_PATCH_ROWS; c2 * MEAS_PATCH_ROWS < b.b2; ++c2)
+                        for (int c3 = 0; c3 < nb3; ++c3) tiles.push_back(make_int4(i, t, (x1 * nb2 + c2) * nb3 + c3, 0));
+        return;
+    }
     for (const SiteBlock& b : site_blocks(g, budget, bytes_per_site))
         for (int t = 0; t < g.n[0]; ++t)
             for (long long x1 = b.a1; x1 < b.b1; ++x1) {
