@@ -19,6 +19,10 @@
 #include <set>
 #include <vector>
 
+// both measurement geometries are checked: strips by default builds, patches here
+#ifndef LGF_MEAS_PATCH
+#define LGF_MEAS_PATCH 1
+#endif
 #include "lgf_tiles.h"
 
 using namespace lgf;

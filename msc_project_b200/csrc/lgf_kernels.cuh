@@ -297,18 +297,20 @@ __device__ __constant__ int c_plane_nu[6] = {1, 2, 3, 2, 3, 3};
 
 constexpr int MEAS_SITES = 32;  // sites per measurement block (x) ; planes in y
 
-// Measurement tile geometry.  A tile's 32 sites are a patch of 4 x2 rows by 8
-// x3 positions at fixed (x0, x1) when N2 % 4 == 0 and N3 % 8 == 0, else 32
-// consecutive sites of the slice (a strip).  The patch keeps the +-3 stencil of
-// the six planes compact: a strip along x3 touches ~5500 distinct sites per
-// tile, a 4 x 8 patch ~3600, and each warp load still covers four whole
-// 128-byte lines (8 consecutive sites per row).  Chunk c of a slice is patch
+// Measurement tile geometry.  A tile's 32 sites are 32 consecutive sites of
+// the slice (a strip), or, built with -DLGF_MEAS_PATCH=1, a patch of 4 x2 rows
+// by 8 x3 positions at fixed (x0, x1) when N2 % 4 == 0 and N3 % 8 == 0.  The
+// patch keeps the +-3 stencil of the six planes compact (a strip along x3
+// touches ~5500 distinct sites per tile, a 4 x 8 patch ~3600) and each warp
+// load still covers four whole 128-byte lines, but measured on one B200 it
+// is 2-8% slower in FP64 (16^4 to 48^4), 4-6% faster in FP32 up to 32^4 and
+// 13% slower on 48^4, so strips are the default.  Chunk c of a slice is patch
 // (x1, b2, b3) = (c / (nb2 nb3), (c / nb3) % nb2, c % nb3); a slice has
-// Vs / 32 chunks either way.  A fixed function of the lattice shape, so the
-// grouping of the partial sums (and every result bit) does not depend on tile
-// shapes or batch partners.
+// Vs / 32 chunks either way.  The geometry is a fixed function of the
+// lattice shape, so the grouping of the partial sums (and every result bit)
+// does not depend on tile shapes or batch partners.
 #ifndef LGF_MEAS_PATCH
-#define LGF_MEAS_PATCH 1
+#define LGF_MEAS_PATCH 0
 #endif
 constexpr int MEAS_PATCH_ROWS = 4, MEAS_PATCH_COLS = 8;
 __host__ __device__ __forceinline__ bool meas_patched(const Geom& g) {
