@@ -235,9 +235,23 @@ template <typename R> struct Plane {
     }
 };
 
+// Where a measurement thread keeps its two 8-coordinate sums: registers, or
+// (LGF_MEAS_SMEM_ACC, double only) its own column of shared memory, which
+// frees 32 registers in the chain-heavy FP64 kernel.  Same operations either way.
+template <typename R> struct RegAcc {
+    alg<R>& a;
+    __device__ __forceinline__ R get(int k) const { return a.v[k]; }
+    __device__ __forceinline__ void set(int k, R x) { a.v[k] = x; }
+};
+template <typename R> struct SmemAcc {
+    R* p;  // coordinate k at p[k * MEAS_ACC_STRIDE]
+    __device__ __forceinline__ R get(int k) const;
+    __device__ __forceinline__ void set(int k, R x);
+};
+
 // F += c * F[A B^dag] without forming the product: only the entries the
 // projection reads (Im of the diagonal, both triangles) are computed.
-template <typename R> __device__ __forceinline__ void leaf_acc(const su3<R>& A, const su3<R>& B, R c, alg<R>& F) {
+template <typename R, typename Acc> __device__ __forceinline__ void leaf_acc(const su3<R>& A, const su3<R>& B, R c, Acc F) {
     // W_ij = sum_k A_ik conj(B_jk)
     R d[3];
 #pragma unroll
@@ -248,8 +262,8 @@ template <typename R> __device__ __forceinline__ void leaf_acc(const su3<R>& A, 
         d[i] = im;
     }
     const R tr = (d[0] + d[1] + d[2]) * R(1.0 / 3.0);
-    F.v[0] = fma(c, d[0] - tr, F.v[0]);
-    F.v[1] = fma(c, d[1] - tr, F.v[1]);
+    F.set(0, fma(c, d[0] - tr, F.get(0)));
+    F.set(1, fma(c, d[1] - tr, F.get(1)));
     const int I[3] = {0, 0, 1}, J[3] = {1, 2, 2};
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
@@ -262,8 +276,8 @@ template <typename R> __device__ __forceinline__ void leaf_acc(const su3<R>& A, 
         wji = cfmac(A.m[3 * j + 2], B.m[3 * i + 2], wji);
         // (-i/2)(a + ib) = (b/2, -a/2),  a + ib = W_ij - conj(W_ji)
         const R a = wij.re - wji.re, b = wij.im + wji.im;
-        F.v[2 + 2 * o] = fma(R(0.5) * c, b, F.v[2 + 2 * o]);
-        F.v[3 + 2 * o] = fma(R(-0.5) * c, a, F.v[3 + 2 * o]);
+        F.set(2 + 2 * o, fma(R(0.5) * c, b, F.get(2 + 2 * o)));
+        F.set(3 + 2 * o, fma(R(-0.5) * c, a, F.get(3 + 2 * o)));
     }
 }
 
@@ -324,6 +338,14 @@ __host__ __device__ __forceinline__ int meas_site_offset(const Geom& g, bool pat
     return (x1 * g.n[2] + b2 * MEAS_PATCH_ROWS + l / MEAS_PATCH_COLS) * g.n[3] + b3 * MEAS_PATCH_COLS +
            l % MEAS_PATCH_COLS;
 }
+#ifndef LGF_MEAS_SMEM_ACC
+#define LGF_MEAS_SMEM_ACC 0
+#endif
+constexpr int MEAS_ACC_STRIDE = MEAS_SITES * 12;  // one column per thread of a 12-warp block
+template <typename R> __device__ __forceinline__ R SmemAcc<R>::get(int k) const { return p[k * MEAS_ACC_STRIDE]; }
+template <typename R> __device__ __forceinline__ void SmemAcc<R>::set(int k, R x) { p[k * MEAS_ACC_STRIDE] = x; }
+template <typename R> constexpr bool meas_smem_acc() { return LGF_MEAS_SMEM_ACC && sizeof(R) == sizeof(double); }
+
 constexpr int MEAS_QSPLIT = LGF_MEAS_QSPLIT;
 constexpr int MEAS_WARPS = 6 * MEAS_QSPLIT;  // warp y: plane y % 6, quadrants of part y / 6
 // resident measurement blocks per SM the launch bounds ask for (caps the
@@ -341,6 +363,7 @@ template <typename R, bool OUT> struct MeasSmem {
             alg<R> Fh[6][MEAS_SITES];
         } part;
     };
+    R acc[meas_smem_acc<R>() ? 16 : 1][meas_smem_acc<R>() ? MEAS_ACC_STRIDE : 1];  // G, Fhat columns (LGF_MEAS_SMEM_ACC)
     alg<R> F[6][MEAS_SITES];          // improved F per plane
     alg<R> C[OUT ? 6 : 1][MEAS_SITES];  // clover F per plane (single-lattice passes only)
     double E[6][MEAS_SITES];
@@ -381,10 +404,10 @@ __device__ __forceinline__ su3<R> load_line(const MeasSmem<R, OUT>* sm, int sdir
 // quadrant): G = the sum of the 1x1 leaves' projections, Fhat = the weighted
 // sum of the other shapes' (see the comment above Plane for the leaf
 // decomposition).  The clover F is G/4 and the improved F is Fhat + 19/36 G.
-template <typename R, bool OUT>
-__device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+template <typename R, bool OUT, typename Acc>
+__device__ __forceinline__ void plane_fields_body(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                   int mu, int nu, const MeasSmem<R, OUT>* sm, int lane, int qa, int qb,
-                                                  alg<R>& G, alg<R>& Fhat) {
+                                                  Acc G, Acc Fhat) {
     Plane<R> P;
     P.U = U;
     P.V = g.V;
@@ -396,8 +419,8 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
     const R k12 = R(-4.0 / 45.0), k13 = R(1.0 / 120.0), k22 = R(1.0 / 144.0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        G.v[k] = R(0);
-        Fhat.v[k] = R(0);
+        G.set(k, R(0));
+        Fhat.set(k, R(0));
     }
 #pragma unroll 1
     for (int q = qa; q < qb; ++q) {
@@ -463,6 +486,24 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
             P.ext(Pm, qm, false, sn);  // Pm(2,2)
             leaf_acc(Pn, Pm, sg * k22, Fhat);
         }
+    }
+}
+
+template <typename R, bool OUT>
+__device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
+                                                  int mu, int nu, MeasSmem<R, OUT>* sm, int lane, int qa, int qb,
+                                                  alg<R>& Greg, alg<R>& Fhreg) {
+    if constexpr (meas_smem_acc<R>()) {
+        R* col = &sm->acc[0][threadIdx.y * MEAS_SITES + lane];
+        const SmemAcc<R> G{col}, Fhat{col + 8 * MEAS_ACC_STRIDE};
+        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, G, Fhat);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            Greg.v[k] = G.get(k);
+            Fhreg.v[k] = Fhat.get(k);
+        }
+    } else {
+        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, RegAcc<R>{Greg}, RegAcc<R>{Fhreg});
     }
 }
 
