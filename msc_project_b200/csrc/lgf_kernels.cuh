@@ -65,14 +65,14 @@ __device__ __forceinline__ su3<R> staple_sum(const cplx<R>* __restrict__ U, cons
         {
             su3<R> a2 = load_link(U, V, nu, s);
             su3<R> a3 = load_link(U, V, mu, xpn);
-            su3<R> t = mul_nn(a2, a3);
+            su3<R> t = mul_nn_su3(a2, a3);
             su3<R> a1 = load_link(U, V, nu, xpm);
             acc_na(S, a1, t);
         }
         {
             su3<R> b1 = load_link(U, V, mu, xmn);
             su3<R> b2 = load_link(U, V, nu, xmnpm);
-            su3<R> t = mul_nn(b1, b2);
+            su3<R> t = mul_nn_su3(b1, b2);
             su3<R> b3 = load_link(U, V, nu, xmn);
             acc_an(S, t, b3);
         }
@@ -80,13 +80,47 @@ __device__ __forceinline__ su3<R> staple_sum(const cplx<R>* __restrict__ U, cons
     return S;
 }
 
+#ifndef LGF_TA_ONLY
+#define LGF_TA_ONLY 1  // the force's product forms only the entries its projection reads
+#endif
+// ta_part(A B, s) computing only what the projection reads: the imaginary
+// parts of the diagonal and the three off-diagonal pairs (90 real
+// operations instead of 108 for the full product)
+template <typename R> __device__ __forceinline__ alg<R> ta_of_product(const su3<R>& A, const su3<R>& B, R s) {
+    R d[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R im = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) im = fma(A.m[3 * i + k].re, B.m[3 * k + i].im, fma(A.m[3 * i + k].im, B.m[3 * k + i].re, im));
+        d[i] = R(2) * im;
+    }
+    const R tr = (d[0] + d[1] + d[2]) * R(1.0 / 3.0);
+    alg<R> z;
+    z.v[0] = s * (d[0] - tr);
+    z.v[1] = s * (d[1] - tr);
+    const int I[3] = {0, 0, 1}, J[3] = {1, 2, 2};
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        const int i = I[o], j = J[o];
+        cplx<R> wij = cmul(A.m[3 * i], B.m[j]);
+        wij = cfma(A.m[3 * i + 1], B.m[3 + j], wij);
+        wij = cfma(A.m[3 * i + 2], B.m[6 + j], wij);
+        cplx<R> wji = cmul(A.m[3 * j], B.m[i]);
+        wji = cfma(A.m[3 * j + 1], B.m[3 + i], wji);
+        wji = cfma(A.m[3 * j + 2], B.m[6 + i], wji);
+        z.v[2 + 2 * o] = s * (wij.re - wji.re);
+        z.v[3 + 2 * o] = s * (wij.im + wji.im);
+    }
+    return z;
+}
+
 template <typename R>
 __device__ __forceinline__ alg<R> flow_gradient(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                 int mu, su3<R>& u_out) {
     const su3<R> S = staple_sum<R>(U, g, s, c, mu);
     u_out = load_link(U, g.V, mu, s);
-    const su3<R> W = mul_nn(u_out, S);
-    return ta_part(W, R(-0.5));
+    return LGF_TA_ONLY ? ta_of_product(u_out, S, R(-0.5)) : ta_part(mul_nn(u_out, S), R(-0.5));
 }
 
 // Device descriptor of one resident lattice.  Every flow launch works on a
@@ -153,6 +187,8 @@ __global__ void __launch_bounds__(StageMaxThreads<R>::value, LGF_STAGE_MINB) k_r
             X = alg_scale(eps, dd);
         }
         const su3<R> E = expm_alg(X);
+        // the stored link is the full product (rebuilding its third row from
+        // the first two would let their rounding drift into it step after step)
         store_link(Uout, g.V, mu, s, mul_nn(E, u));
     }
 }
