@@ -212,6 +212,10 @@ __global__ void __launch_bounds__(StageMaxThreads<R>::value, LGF_STAGE_MINB) k_r
 // instead of 34 and 40 for separate loops.
 struct PlanePos { int s, xm, xn; };
 
+#ifndef LGF_MEAS_ROW3
+#define LGF_MEAS_ROW3 1  // path products of the measurement rebuild their third row (mul_nn_su3)
+#endif
+
 template <typename R> struct Plane {
     const cplx<R>* __restrict__ U;
     int V, mu, nu;
@@ -261,12 +265,12 @@ template <typename R> struct Plane {
             const su3<R> l = load_link(U, V, dir, p.s);
             p.s = (xc == d.n - 1) ? p.s - (d.n - 1) * d.stride : p.s + d.stride;
             xc = wrap_inc(xc, d.n);
-            P = mul_nn(P, l);
+            P = LGF_MEAS_ROW3 ? mul_nn_su3(P, l) : mul_nn(P, l);
         } else {
             p.s = (xc == 0) ? p.s + (d.n - 1) * d.stride : p.s - d.stride;
             xc = wrap_dec(xc, d.n);
             const su3<R> l = load_link(U, V, dir, p.s);
-            P = mul_na(P, l);
+            P = LGF_MEAS_ROW3 ? mul_na_su3(P, l) : mul_na(P, l);
         }
     }
 };

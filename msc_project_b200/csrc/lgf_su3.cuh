@@ -143,13 +143,14 @@ template <typename R> __device__ __forceinline__ void acc_an(su3<R>& acc, const 
 }
 
 #ifndef LGF_SU3_ROW3
-#define LGF_SU3_ROW3 1  // the staple's link-link products take their third row as conj(r0 x r1)
+#define LGF_SU3_ROW3 1  // products of links that feed the force or a measurement: third row as conj(r0 x r1)
 #endif
 // c = a * b for a, b in SU(3): rows 0 and 1 as products, row 2 as
 // conj(r0 x r1), which for a unitary product with det 1 is the same row
 // (96 real operations instead of 108; equal to rounding on SU(3) inputs).
-// Used for the staple's intermediate products, which only feed the force;
-// a stored link is never built this way.
+// Used for the staple's intermediate products, which only feed the force,
+// and for the measurement's path products; a stored link is never built
+// this way.
 template <typename R> __device__ __forceinline__ su3<R> mul_nn_su3(const su3<R>& a, const su3<R>& b) {
     if (!LGF_SU3_ROW3) return mul_nn(a, b);
     su3<R> c;
@@ -162,6 +163,27 @@ template <typename R> __device__ __forceinline__ su3<R> mul_nn_su3(const su3<R>&
             c.m[3 * r + col] = cfma(a.m[3 * r + 2], b.m[6 + col], s);
         }
     // conj(r0 x r1): (r0_1 r1_2 - r0_2 r1_1, r0_2 r1_0 - r0_0 r1_2, r0_0 r1_1 - r0_1 r1_0)*
+    const cplx<R> x0 = csub(cmul(c.m[1], c.m[5]), cmul(c.m[2], c.m[4]));
+    const cplx<R> x1 = csub(cmul(c.m[2], c.m[3]), cmul(c.m[0], c.m[5]));
+    const cplx<R> x2 = csub(cmul(c.m[0], c.m[4]), cmul(c.m[1], c.m[3]));
+    c.m[6] = cmk<R>(x0.re, -x0.im);
+    c.m[7] = cmk<R>(x1.re, -x1.im);
+    c.m[8] = cmk<R>(x2.re, -x2.im);
+    return c;
+}
+
+// c = a * b^dag for a, b in SU(3), the third row rebuilt as in mul_nn_su3
+template <typename R> __device__ __forceinline__ su3<R> mul_na_su3(const su3<R>& a, const su3<R>& b) {
+    if (!LGF_SU3_ROW3) return mul_na(a, b);
+    su3<R> c;
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            cplx<R> s = cmulc(a.m[3 * r], b.m[3 * col]);
+            s = cfmac(a.m[3 * r + 1], b.m[3 * col + 1], s);
+            c.m[3 * r + col] = cfmac(a.m[3 * r + 2], b.m[3 * col + 2], s);
+        }
     const cplx<R> x0 = csub(cmul(c.m[1], c.m[5]), cmul(c.m[2], c.m[4]));
     const cplx<R> x1 = csub(cmul(c.m[2], c.m[3]), cmul(c.m[0], c.m[5]));
     const cplx<R> x2 = csub(cmul(c.m[0], c.m[4]), cmul(c.m[1], c.m[3]));
