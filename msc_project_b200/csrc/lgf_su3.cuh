@@ -251,15 +251,44 @@ template <typename R> __device__ __forceinline__ herm_d herm_from_alg(const alg<
 // Series form used below c1 = 0.25 (eigenvalues |lambda| <= 2 sqrt(c1/3) < 0.58):
 // with Q^3 = c1 Q + c0 (Cayley-Hamilton), Q^n = a_n + b_n Q + d_n Q^2 where
 // a_{n+1} = c0 d_n, b_{n+1} = a_n + c1 d_n, d_{n+1} = b_n, and
-// f_j = sum_n i^n {a,b,d}_n / n!.  17 terms leave a remainder below 1e-19, so
-// it agrees with the closed form to rounding while needing no transcendental
+// f_j = sum_n i^n {a,b,d}_n / n!.  17 terms leave a remainder below 1e-19 for
+// every c1 < 0.25; fewer suffice for smaller c1 (ch_series_terms), so it
+// agrees with the closed form to rounding while needing no transcendental
 // function (the flow's exponents are small: c1 is ~1e-5..1e-2 at eps = 0.01).
+#ifndef LGF_CH_TERMS
+#define LGF_CH_TERMS 1  // the series stops at the first term count whose tail bound is below 1e-17
+#endif
+// Terms the series needs for c1: the truncated series is the same polynomial
+// in Q, so its error in operator norm is the exponential's tail,
+// rho^(N+1)/(N+1)! * 2 with rho^2 = 4 c1 / 3 the largest |eigenvalue|^2;
+// N terms keep it below 1e-17 for c1 below these bounds (compared through
+// the high word of the non-negative double c1, an integer comparison: a
+// smaller high word means a smaller value).
+__device__ __forceinline__ int ch_series_terms(double c1) {
+    if (!LGF_CH_TERMS) return 17;
+    const int hi = __double2hiint(c1);
+    return hi < 0x3ee818a5 ? 5    // c1 < 1.149e-5
+         : hi < 0x3f1999da ? 6    // 9.766e-5
+         : hi < 0x3f407746 ? 7    // 5.025e-4
+         : hi < 0x3f5e3864 ? 8    // 1.8445e-3
+         : hi < 0x3f75d5da ? 9    // 5.3309e-3
+         : hi < 0x3f8a78af ? 10   // 1.29255e-2
+         : hi < 0x3f9c1765 ? 11   // 2.7433e-2
+         : hi < 0x3faae18a ? 12   // 5.2502e-2
+         : hi < 0x3fb7b1af ? 13   // 9.2555e-2
+         : hi < 0x3fc38b04 ? 14   // 0.15268
+         : hi < 0x3fce877e ? 15   // 0.23851
+                           : 17;
+}
+
 __device__ __forceinline__ void ch_series(double c0, double c1, cplx<double>& f0, cplx<double>& f1,
                                           cplx<double>& f2) {
     double a = 1.0, b = 0.0, d = 0.0, inv = 1.0;
     double r0 = 1.0, i0 = 0.0, r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
+    const int nterms = ch_series_terms(c1);
 #pragma unroll
     for (int n = 1; n <= 17; ++n) {
+        if (n > nterms) break;
         const double an = c0 * d, bn = fma(c1, d, a);
         d = b;
         a = an;
