@@ -3,7 +3,9 @@
 //
 // On a lattice of the job's own shape (generated links; the volume decides
 // which orders keep the stencil's neighbours in L1/L2), candidates are timed
-// with CUDA events on the context's stream, one parameter at a time:
+// with CUDA events on the context's stream (each over at least ~20 ms of
+// launches; a candidate must beat the current shape by 2%), one parameter at
+// a time:
 //   stage:       block size {128, 256, 384},
 //                then the tile order {x1 columns per CTA, row blocks through
 //                x0}, then (row blocks) the block budget {2, 8, 32 MB};
@@ -13,6 +15,7 @@
 // No candidate changes a result: only block shapes and tile order differ.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <memory>
 #include <vector>
 
@@ -69,14 +72,21 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
     TileShape cur = default_shape(prec);
     float cur_ms = 0.f;
     const double MB = double(1 << 20);
+    // A candidate replaces the current shape only when it is more than 2%
+    // faster, each timed over at least ~20 ms of launches: the clock of a
+    // power-capped GPU wanders by about that much, and a shape chosen on
+    // noise would follow the volume class everywhere.
+    const float KEEP = 0.98f, TARGET_MS = 20.f;
     // ---- RK3 stage: one step (three stage launches) per repetition
-    const int reps = b.g.V >= (1 << 20) ? 3 : 10;
+    float probe = 0.f;
+    if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, -1, 1, &probe);
+    const int reps = std::max(3, std::min(200, (int)(TARGET_MS / std::max(probe, 1e-3f))));
     if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, -1, reps, &cur_ms);
     auto try_stage = [&](TileShape t) {
         if (rc != LGF_OK || t == cur) return;
         float ms = 0.f;
         rc = time_shape(ctx, prec, b, t, -1, reps, &ms);
-        if (rc == LGF_OK && ms < cur_ms) {
+        if (rc == LGF_OK && ms < KEEP * cur_ms) {
             cur = t;
             cur_ms = ms;
         }
@@ -100,12 +110,14 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
         }
     // ---- measurement kernel alone
     float meas_ms = 0.f;
-    if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, 3, reps, &meas_ms);
+    if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, 3, 1, &probe);
+    const int mreps = std::max(3, std::min(200, (int)(TARGET_MS / std::max(probe, 1e-3f))));
+    if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, 3, mreps, &meas_ms);
     auto try_meas = [&](TileShape t) {
         if (rc != LGF_OK || t == cur) return;
         float ms = 0.f;
-        rc = time_shape(ctx, prec, b, t, 3, reps, &ms);
-        if (rc == LGF_OK && ms < meas_ms) {
+        rc = time_shape(ctx, prec, b, t, 3, mreps, &ms);
+        if (rc == LGF_OK && ms < KEEP * meas_ms) {
             cur = t;
             meas_ms = ms;
         }
