@@ -57,7 +57,7 @@ BYTES_PER_SITE_STAGE = {0: 4480.0 / 3, 1: 2240.0 / 3}
 FLOPS_PER_SITE_STAGE = 42888.0 / 3
 # DRAM traffic of one stage launch from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum), scaled to this workload; see profiles/.
-NCU_STAGE_TRAFFIC_BYTES = {0: 1121.2e6, 1: 539.4e6}  # stage-2 launch; profiles/k_rk3_stage_*_24x24x24x48.md
+NCU_STAGE_TRAFFIC_BYTES = {0: 1111.5e6, 1: 534.9e6}  # stage-2 launch; profiles/k_rk3_stage_*_24x24x24x48.md
 FP64_FMA_PER_SM_PER_CLK = 64  # B200: 64 FP64 FMA lanes per SM (nominal)
 FP32_FMA_PER_SM_PER_CLK = 128  # B200: 128 FP32 FMA lanes per SM (nominal)
 N_SM = 148
