@@ -163,7 +163,10 @@ int run_wave(lgf_ctx* ctx, int prec, std::vector<JobRun*>& runs, GroupBase* grp,
 
 // L2-sized waves: jobs sorted by volume, packed greedily while the wave's
 // per-stage working set fits the budget; order inside a wave is the input order.
-const size_t L2_WAVE_BYTES = 96u << 20;
+#ifndef LGF_BATCH_WAVE_MB
+#define LGF_BATCH_WAVE_MB 96  // 0: every job of a precision in one wave
+#endif
+const size_t L2_WAVE_BYTES = (size_t)LGF_BATCH_WAVE_MB << 20;
 
 std::vector<std::vector<JobRun*>> l2_waves(const std::vector<JobRun*>& jobs, int prec) {
     const size_t rs = prec == LGF_PREC_FP64 ? 8 : 4;
@@ -174,7 +177,7 @@ std::vector<std::vector<JobRun*>> l2_waves(const std::vector<JobRun*>& jobs, int
     size_t cur = 0;
     for (JobRun* r : order) {
         const size_t b = stage_bytes(r);
-        if (waves.empty() || cur + b > L2_WAVE_BYTES) {
+        if (waves.empty() || (L2_WAVE_BYTES > 0 && cur + b > L2_WAVE_BYTES)) {
             waves.emplace_back();
             cur = 0;
         }
@@ -253,7 +256,7 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
             max_tiles = std::max(max_tiles, t);
             max_members = std::max(max_members, (int)wave.size());
         }
-        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shapes[prec], max_members, max_tiles, true));
+        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shapes[prec], max_members, max_tiles, true, true));
         if (!grp) {
             rc = ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
             break;

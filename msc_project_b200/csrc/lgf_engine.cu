@@ -11,6 +11,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "lgf_engine.cuh"
@@ -238,12 +239,16 @@ __global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ 
 
 static inline size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
 
+#ifndef LGF_STAGE_CARVEOUT
+#define LGF_STAGE_CARVEOUT -1  // preferred shared-memory carveout of the stage kernels in percent; -1: the driver's
+#endif
+
 // ------------------------------------------------------------------ groups
 template <typename R> class Group : public GroupBase {
 public:
-    Group(lgf_ctx* ctx, const TileShape& shape, int max_members, long long max_tiles, bool dynamic)
+    Group(lgf_ctx* ctx, const TileShape& shape, int max_members, long long max_tiles, bool dynamic, bool per_volume)
         : ctx_(ctx), shape_(shape), threads_(shape.threads), max_members_(max_members), max_tiles_(max_tiles),
-          dynamic_(dynamic) {}
+          dynamic_(dynamic), per_volume_(per_volume) {}
     ~Group() override {
         cudaStreamSynchronize(ctx_->stream);  // the lists are in use until then
         if (step_exec_) cudaGraphExecDestroy(step_exec_);
@@ -264,6 +269,11 @@ public:
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_counts_, sizeof(int) * 4));
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_sel_, sizeof(int) * (SEL_HEADER + SEL_FIELDS * (size_t)max_members_)));
         LGF_CUDA_TRY(ctx_, cudaMemsetAsync(d_counts_, 0, sizeof(int) * 4, ctx_->stream));
+#if LGF_STAGE_CARVEOUT >= 0
+        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
+        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
+        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
+#endif
         int nb = 0;
         LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rk3_stage<R, 1>, threads_, 0));
         stage_grid_max_ = std::max(1, nb) * ctx_->sm_count;
@@ -316,11 +326,12 @@ public:
             d.eps = (R)b.eps;
             // a tile is threads_/4 consecutive sites with all four link directions;
             // per site a stage reads and writes 4 links and 4 su(3) accumulators
-            if (!(shape_.stage_order == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
-                append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, shape_.stage_budget, 4.0 * (2 * 18 + 8) * sizeof(R));
+            const TileShape ls = list_shape(b.g.V);
+            if (!(ls.stage_order == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
+                append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, ls.stage_budget, 4.0 * (2 * 18 + 8) * sizeof(R));
             // this member's segment of the measurement list
             seg_off_[i] = (int)mtiles.size();
-            append_measure_tiles(mtiles, (int)i, b.g, shape_.meas_budget, 4.0 * 18 * sizeof(R));
+            append_measure_tiles(mtiles, (int)i, b.g, ls.meas_budget, 4.0 * 18 * sizeof(R));
             seg_len_[i] = (int)mtiles.size() - seg_off_[i];
         }
         if ((long long)tiles.size() > max_tiles_)
@@ -536,12 +547,25 @@ private:
         return LGF_OK;
     }
 
+    // The work order (tile order and block budgets) of one member's lists.
+    // The group's shape fixes the kernels (block size, measurement split);
+    // in a group of uneven volumes (per_volume_: batches, serving) each
+    // member is ordered as tuned for its own volume class, else by the
+    // defaults -- an order tuned on 24^3x48 (whole-slice measurement blocks)
+    // costs a 48^4 member 40% in the measurement.
+    TileShape list_shape(long long V) const {
+        if (!per_volume_) return shape_;
+        const int prec = std::is_same<R, double>::value ? LGF_PREC_FP64 : LGF_PREC_FP32MIXED;
+        return has_tuned(ctx_, prec, V) ? tuned_shape(ctx_, prec, V) : default_shape(prec);
+    }
+
     lgf_ctx* ctx_;
     TileShape shape_;
     int threads_;
     int max_members_;
     long long max_tiles_;
     bool dynamic_;
+    bool per_volume_;
     std::vector<LatticeBuf*> members_;
     std::vector<LatDesc<R>> h_desc_;
     std::vector<int> seg_off_, seg_len_;  // each member's segment of d_all_mtiles_
@@ -561,7 +585,7 @@ private:
 };
 
 GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
-                      bool dynamic) {
+                      bool dynamic, bool per_volume) {
     if (shape.threads < 128 || shape.threads % 128 || shape.threads > stage_max_threads(precision) ||
         (shape.meas_split != 1 && shape.meas_split != 2) || shape.stage_budget <= 0 || shape.meas_budget <= 0) {
         set_error(ctx, LGF_EINVAL, "invalid tile shape (threads %d, measurement split %d)", shape.threads,
@@ -570,11 +594,11 @@ GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int m
     }
     GroupBase* g = nullptr;
     if (precision == LGF_PREC_FP64) {
-        auto* p = new (std::nothrow) Group<double>(ctx, shape, max_members, max_tiles, dynamic);
+        auto* p = new (std::nothrow) Group<double>(ctx, shape, max_members, max_tiles, dynamic, per_volume);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     } else {
-        auto* p = new (std::nothrow) Group<float>(ctx, shape, max_members, max_tiles, dynamic);
+        auto* p = new (std::nothrow) Group<float>(ctx, shape, max_members, max_tiles, dynamic, per_volume);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     }

@@ -184,8 +184,10 @@ public:
     virtual const TileShape& shape() const = 0;
 };
 
+// dynamic: members change after the graphs are captured; per_volume: each
+// member's lists follow the work order tuned for its own volume class
 GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
-                      bool dynamic);
+                      bool dynamic, bool per_volume = false);
 
 int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b);
 int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file_order);

@@ -208,8 +208,9 @@ __global__ void __launch_bounds__(StageMaxThreads<R>::value, LGF_STAGE_MINB) k_r
 //      C11 = 1/4 (1x1), C22 = 1/4 (2x2), C12 = 1/8 (1x2 + 2x1), C13 = 1/8 (1x3 + 3x1)
 // (SU3_field.cpp:588-597), and the clover F = F[C11] for E.  The paths are
 // built as shared chains (a path of a shape extends the path of the shape
-// before it by one link), 27 matrix products and 27 link loads per quadrant
-// instead of 34 and 40 for separate loops.
+// before it by one link) and from shared straight lines: 12 matrix products
+// and 14 global link loads per quadrant (plane_fields_body) instead of 34 and
+// 40 for separate loops.
 struct PlanePos { int s, xm, xn; };
 
 #ifndef LGF_MEAS_ROW3
@@ -389,6 +390,35 @@ template <typename R> __device__ __forceinline__ R SmemAcc<R>::get(int k) const 
 template <typename R> __device__ __forceinline__ void SmemAcc<R>::set(int k, R x) { p[k * MEAS_ACC_STRIDE] = x; }
 template <typename R> constexpr bool meas_smem_acc() { return LGF_MEAS_SMEM_ACC && sizeof(R) == sizeof(double); }
 
+// A path matrix parked in the thread's own shared-memory column until it is
+// extended by one more link.  Only its first two rows are kept when the
+// extension rebuilds the third (mul_nn_su3 / mul_na_su3 read rows 0 and 1 of
+// their left operand), so a parked path is exactly the one put there.
+constexpr int MEAS_STASH_ENTRIES = LGF_MEAS_ROW3 ? 6 : 9;
+template <typename R> struct PathStash {
+    typename vec2_of<R>::type* p;  // entry k at p[k * MEAS_ACC_STRIDE]
+    __device__ __forceinline__ void put(const su3<R>& P) const {
+#pragma unroll
+        for (int k = 0; k < MEAS_STASH_ENTRIES; ++k) {
+            p[k * MEAS_ACC_STRIDE].x = P.m[k].re;
+            p[k * MEAS_ACC_STRIDE].y = P.m[k].im;
+        }
+    }
+    __device__ __forceinline__ su3<R> get() const {
+        su3<R> P;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (k < MEAS_STASH_ENTRIES) {
+                const typename vec2_of<R>::type v = p[k * MEAS_ACC_STRIDE];
+                P.m[k] = cmk<R>(v.x, v.y);
+            } else {
+                P.m[k] = cmk<R>(R(0), R(0));  // never read: the next product rebuilds the row
+            }
+        }
+        return P;
+    }
+};
+
 constexpr int MEAS_QSPLIT = LGF_MEAS_QSPLIT;
 constexpr int MEAS_WARPS = 6 * MEAS_QSPLIT;  // warp y: plane y % 6, quadrants of part y / 6
 // resident measurement blocks per SM the launch bounds ask for (caps the
@@ -407,6 +437,7 @@ template <typename R, bool OUT> struct MeasSmem {
         } part;
     };
     R acc[meas_smem_acc<R>() ? 16 : 1][meas_smem_acc<R>() ? MEAS_ACC_STRIDE : 1];  // G, Fhat columns (LGF_MEAS_SMEM_ACC)
+    typename vec2_of<R>::type stash[2][MEAS_STASH_ENTRIES][MEAS_ACC_STRIDE];  // two paths per thread (PathStash)
     alg<R> F[6][MEAS_SITES];          // improved F per plane
     alg<R> C[OUT ? 6 : 1][MEAS_SITES];  // clover F per plane (single-lattice passes only)
     double E[6][MEAS_SITES];
@@ -442,15 +473,30 @@ __device__ __forceinline__ su3<R> load_line(const MeasSmem<R, OUT>* sm, int sdir
     return L;
 }
 
+#ifndef LGF_MEAS_REUSE
+#define LGF_MEAS_REUSE 1  // paths extended from parked shorter paths: 12 products per quadrant instead of 15
+#endif
+
 // Quadrants [qa, qb) of plane (mu, nu) at the thread's site, using the
-// block's shared lines (21 matrix products and 16 global link loads per
-// quadrant): G = the sum of the 1x1 leaves' projections, Fhat = the weighted
-// sum of the other shapes' (see the comment above Plane for the leaf
-// decomposition).  The clover F is G/4 and the improved F is Fhat + 19/36 G.
+// block's shared lines: G = the sum of the 1x1 leaves' projections, Fhat =
+// the weighted sum of the other shapes' (see the comment above Plane for the
+// leaf decomposition).  The clover F is G/4 and the improved F is
+// Fhat + 19/36 G.  With a b-fold path written as its steps (n = sn nu,
+// m = sm mu), the twelve paths of a quadrant are
+//   Pn(a,1) = n m^a        (a chain: each extends the one before by m)
+//   Pm(1,b) = m n^b        (a chain along n)
+//   Pm(a,1) = line_m(a) n,  Pn(1,b) = line_n(b) m   (from the shared lines)
+//   Pn(2,2) = Pn(1,2) m,    Pm(2,2) = Pm(2,1) n
+// 12 matrix products and 14 global link loads per quadrant; the paths that
+// are extended after other work are parked in the thread's shared-memory
+// column (PathStash: Pm(1,1), Pm(2,1), Pn(1,2)), and the leaves are added in
+// the order (1,1) | (2,1), (3,1), (1,2), (1,3), (2,2), the order of the
+// 15-product form (LGF_MEAS_REUSE=0), whose every product it repeats: both
+// give the same bits.
 template <typename R, bool OUT, typename Acc>
 __device__ __forceinline__ void plane_fields_body(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                   int mu, int nu, const MeasSmem<R, OUT>* sm, int lane, int qa, int qb,
-                                                  Acc G, Acc Fhat) {
+                                                  Acc G, Acc Fhat, PathStash<R> sa, PathStash<R> sb) {
     Plane<R> P;
     P.U = U;
     P.V = g.V;
@@ -471,6 +517,55 @@ __device__ __forceinline__ void plane_fields_body(const cplx<R>* __restrict__ U,
         const int sn = (q == 0 || q == 2) ? 1 : -1;
         const R sg = (q == 0 || q == 3) ? R(1) : R(-1);
         const int sdm = 2 * mu + (sm_ < 0 ? 1 : 0), sdn = 2 * nu + (sn < 0 ? 1 : 0);
+        if (LGF_MEAS_REUSE) {
+            // (1,1)
+            PlanePos pn = x0;
+            su3<R> Pn = P.step(pn, false, sn);
+            P.ext(Pn, pn, true, sm_);  // Pn(1,1)
+            PlanePos pm = x0;
+            su3<R> Pm = P.step(pm, true, sm_);
+            P.ext(Pm, pm, false, sn);  // Pm(1,1), pm at x + m + n
+            leaf_acc(Pn, Pm, sg, G);
+            sa.put(Pm);
+            // (2,1)
+            P.ext(Pn, pn, true, sm_);  // Pn(2,1)
+            PlanePos p21 = x0;
+            P.advance(p21, true, sm_, 2);
+            Pm = load_line(sm, sdm, 2, lane);
+            P.ext(Pm, p21, false, sn);  // Pm(2,1), p21 at x + 2m + n
+            leaf_acc(Pn, Pm, sg * k12, Fhat);
+            sb.put(Pm);
+            // (3,1)
+            P.ext(Pn, pn, true, sm_);  // Pn(3,1)
+            PlanePos p31 = x0;
+            P.advance(p31, true, sm_, 3);
+            Pm = load_line(sm, sdm, 3, lane);
+            P.ext(Pm, p31, false, sn);  // Pm(3,1)
+            leaf_acc(Pn, Pm, sg * k13, Fhat);
+            // (1,2)
+            Pm = sa.get();
+            P.ext(Pm, pm, false, sn);  // Pm(1,2)
+            PlanePos p12 = x0;
+            P.advance(p12, false, sn, 2);
+            Pn = load_line(sm, sdn, 2, lane);
+            P.ext(Pn, p12, true, sm_);  // Pn(1,2), p12 at x + 2n + m
+            leaf_acc(Pn, Pm, sg * k12, Fhat);
+            sa.put(Pn);
+            // (1,3)
+            P.ext(Pm, pm, false, sn);  // Pm(1,3)
+            PlanePos p13 = x0;
+            P.advance(p13, false, sn, 3);
+            Pn = load_line(sm, sdn, 3, lane);
+            P.ext(Pn, p13, true, sm_);  // Pn(1,3)
+            leaf_acc(Pn, Pm, sg * k13, Fhat);
+            // (2,2)
+            Pn = sa.get();
+            P.ext(Pn, p12, true, sm_);  // Pn(2,2)
+            Pm = sb.get();
+            P.ext(Pm, p21, false, sn);  // Pm(2,2)
+            leaf_acc(Pn, Pm, sg * k22, Fhat);
+            continue;
+        }
         // row: (1,1), (2,1), (3,1)
         PlanePos pn = x0;
         su3<R> Rn = P.step(pn, false, sn);
@@ -536,17 +631,19 @@ template <typename R, bool OUT>
 __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U, const Geom& g, int s, const Coord& c,
                                                   int mu, int nu, MeasSmem<R, OUT>* sm, int lane, int qa, int qb,
                                                   alg<R>& Greg, alg<R>& Fhreg) {
+    const int column = threadIdx.y * MEAS_SITES + lane;
+    const PathStash<R> sa{&sm->stash[0][0][column]}, sb{&sm->stash[1][0][column]};
     if constexpr (meas_smem_acc<R>()) {
-        R* col = &sm->acc[0][threadIdx.y * MEAS_SITES + lane];
+        R* col = &sm->acc[0][column];
         const SmemAcc<R> G{col}, Fhat{col + 8 * MEAS_ACC_STRIDE};
-        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, G, Fhat);
+        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, G, Fhat, sa, sb);
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             Greg.v[k] = G.get(k);
             Fhreg.v[k] = Fhat.get(k);
         }
     } else {
-        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, RegAcc<R>{Greg}, RegAcc<R>{Fhreg});
+        plane_fields_body<R, OUT>(U, g, s, c, mu, nu, sm, lane, qa, qb, RegAcc<R>{Greg}, RegAcc<R>{Fhreg}, sa, sb);
     }
 }
 
