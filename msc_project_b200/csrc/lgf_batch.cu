@@ -256,7 +256,8 @@ int lgf_batch_run(lgf_ctx* ctx, lgf_job* jobs, int njobs, lgf_batch_stats* stats
             max_tiles = std::max(max_tiles, t);
             max_members = std::max(max_members, (int)wave.size());
         }
-        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shapes[prec], max_members, max_tiles, true, true));
+        std::unique_ptr<GroupBase> grp(make_group(ctx, prec, shapes[prec], max_members, max_tiles, true, true,
+                                                  std::min(max_members, 32)));
         if (!grp) {
             rc = ctx->err.empty() ? set_error(ctx, LGF_ENOMEM, "group creation failed") : LGF_ECUDA;
             break;

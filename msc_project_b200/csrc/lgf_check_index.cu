@@ -12,7 +12,9 @@
 //     bijections into the padded buffers with 16-byte aligned vector loads;
 //   - the stage and measurement tile lists cover every tile exactly once for
 //     row-block and column orders and a range of budgets and block sizes, and
-//     the measurement's strips or patches cover every site of a slice once.
+//     the measurement's strips or patches cover every site of a slice once;
+//   - the launch segments of a group (member_runs) split a list of members
+//     into at most `slots` back-to-back runs of whole members covering it.
 // Prints one line and exits 0 when everything holds.
 #include <cstdio>
 #include <cstdlib>
@@ -185,7 +187,32 @@ static void check_tiles(const Geom& g) {
     }
 }
 
+static void check_member_runs() {
+    const std::vector<std::vector<int>> lists = {
+        {}, {0}, {5}, {20736}, {43, 43, 43}, {683, 20736, 683, 683, 2048, 165888, 1},
+        std::vector<int>(64, 43), std::vector<int>(16, 20736), {0, 7, 0, 9}};
+    for (const auto& lens : lists)
+        for (int slots : {1, 2, 3, 16, 32})
+            for (long long min_run : {0LL, 1LL, 1184LL, 3552LL, 100000LL}) {
+                const std::vector<int2> runs = member_runs(lens, slots, min_run);
+                CHECK(!runs.empty() && (int)runs.size() <= slots);
+                // runs are back to back, cover the list, and end on member boundaries
+                std::set<long long> bounds;
+                long long acc = 0;
+                bounds.insert(0);
+                for (int t : lens) bounds.insert(acc += t);
+                long long next = 0;
+                for (const int2& r : runs) {
+                    CHECK(r.x == next && r.y >= 0);
+                    next += r.y;
+                    CHECK(bounds.count(next) == 1);
+                }
+                CHECK(next == acc);
+            }
+}
+
 int main() {
+    check_member_runs();
     const int shapes[][4] = {{4, 4, 4, 4}, {4, 6, 8, 10}, {6, 6, 6, 6}, {4, 4, 6, 6}, {8, 4, 6, 4},
                              {10, 4, 4, 8}, {4, 20, 18, 18}, {4, 6, 6, 10}, {4, 6, 8, 16}, {6, 4, 12, 8}};
     int n = 0;

@@ -209,16 +209,19 @@ int count_measurements(const lgf_flow_opts& o) {
 // device from the per-member segments of the group's full measurement tile
 // list (built once per change of members), so that choosing which members a
 // measurement covers is one small copy and this launch, with no host wait.
-//   sel = [nsel, total tiles, total slices,
+//   sel = [nsel, total tiles, total slices, 0,
+//          the launch segments (first tile, tiles) of the measurement kernel,
+//          one pair per launch slot (read by k_measure itself),
 //          then per selected member k: member, segment offset, tiles, first
 //          output tile, N0, first output slice]
 // Outputs: mtiles (the selected segments back to back), rtiles (member, t)
 // for t < N0, jobs[k] = member, counts = {tiles, slices, nsel}.  Grid
 // (max(nsel, 1), any): block (k, y) copies a share of segment k.
-constexpr int SEL_HEADER = 3, SEL_FIELDS = 6;
-__global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ sel, const int4* __restrict__ all,
-                                                        int4* __restrict__ mtiles, int2* __restrict__ rtiles,
-                                                        int* __restrict__ jobs, int* __restrict__ counts) {
+constexpr int SEL_HEADER = 4, SEL_FIELDS = 6;
+__global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ sel, int fields,
+                                                        const int4* __restrict__ all, int4* __restrict__ mtiles,
+                                                        int2* __restrict__ rtiles, int* __restrict__ jobs,
+                                                        int* __restrict__ counts) {
     const int nsel = sel[0];
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
         counts[0] = sel[1];
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ 
     }
     const int k = blockIdx.x;
     if (k >= nsel) return;
-    const int* f = sel + SEL_HEADER + SEL_FIELDS * k;
+    const int* f = sel + fields + SEL_FIELDS * k;
     const int member = f[0], off = f[1], n = f[2], mstart = f[3], n0 = f[4], rstart = f[5];
     for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += gridDim.y * blockDim.x)
         mtiles[mstart + i] = all[off + i];
@@ -239,20 +242,18 @@ __global__ void __launch_bounds__(256) k_select_measure(const int* __restrict__ 
 
 static inline size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
 
-#ifndef LGF_STAGE_CARVEOUT
-#define LGF_STAGE_CARVEOUT -1  // preferred shared-memory carveout of the stage kernels in percent; -1: the driver's
-#endif
 
 // ------------------------------------------------------------------ groups
 template <typename R> class Group : public GroupBase {
 public:
-    Group(lgf_ctx* ctx, const TileShape& shape, int max_members, long long max_tiles, bool dynamic, bool per_volume)
+    Group(lgf_ctx* ctx, const TileShape& shape, int max_members, long long max_tiles, bool dynamic, bool per_volume,
+          int slots)
         : ctx_(ctx), shape_(shape), threads_(shape.threads), max_members_(max_members), max_tiles_(max_tiles),
-          dynamic_(dynamic), per_volume_(per_volume) {}
+          dynamic_(dynamic), per_volume_(per_volume), slots_(std::max(1, std::min(slots, max_members))),
+          step_execs_(slots_ + 1, nullptr), meas_execs_(slots_ + 1, nullptr) {}
     ~Group() override {
         cudaStreamSynchronize(ctx_->stream);  // the lists are in use until then
-        if (step_exec_) cudaGraphExecDestroy(step_exec_);
-        if (meas_exec_) cudaGraphExecDestroy(meas_exec_);
+        drop_graphs();
         cudaFree(d_desc_);
         cudaFree(d_tiles_);
         cudaFree(d_mtiles_);
@@ -260,6 +261,7 @@ public:
         cudaFree(d_rtiles_);
         cudaFree(d_jobs_);
         cudaFree(d_counts_);
+        cudaFree(d_seg_);
         cudaFree(d_sel_);
     }
 
@@ -267,13 +269,11 @@ public:
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_desc_, sizeof(LatDesc<R>) * max_members_));
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_tiles_, sizeof(int2) * max_tiles_));
         LGF_CUDA_TRY(ctx_, cudaMalloc(&d_counts_, sizeof(int) * 4));
-        LGF_CUDA_TRY(ctx_, cudaMalloc(&d_sel_, sizeof(int) * (SEL_HEADER + SEL_FIELDS * (size_t)max_members_)));
+        LGF_CUDA_TRY(ctx_, cudaMalloc(&d_seg_, sizeof(int2) * slots_));
+        LGF_CUDA_TRY(ctx_, cudaMalloc(&d_sel_, sizeof(int) * sel_ints(max_members_)));
         LGF_CUDA_TRY(ctx_, cudaMemsetAsync(d_counts_, 0, sizeof(int) * 4, ctx_->stream));
-#if LGF_STAGE_CARVEOUT >= 0
-        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
-        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
-        LGF_CUDA_TRY(ctx_, cudaFuncSetAttribute(k_rk3_stage<R, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, LGF_STAGE_CARVEOUT));
-#endif
+        LGF_CUDA_TRY(ctx_, cudaMemsetAsync(d_seg_, 0, sizeof(int2) * slots_, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, cudaMemsetAsync(d_sel_, 0, sizeof(int) * sel_ints(max_members_), ctx_->stream));
         int nb = 0;
         LGF_CUDA_TRY(ctx_, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rk3_stage<R, 1>, threads_, 0));
         stage_grid_max_ = std::max(1, nb) * ctx_->sm_count;
@@ -310,6 +310,7 @@ public:
         std::vector<int4> mtiles;
         seg_off_.assign(members.size(), 0);
         seg_len_.assign(members.size(), 0);
+        std::vector<int> stage_len(members.size(), 0);
         for (size_t i = 0; i < members.size(); ++i) {
             const LatticeBuf& b = *members[i];
             LatDesc<R>& d = h_desc_[i];
@@ -327,8 +328,10 @@ public:
             // a tile is threads_/4 consecutive sites with all four link directions;
             // per site a stage reads and writes 4 links and 4 su(3) accumulators
             const TileShape ls = list_shape(b.g.V);
+            const size_t t0 = tiles.size();
             if (!(ls.stage_order == 1 && append_stage_tiles_columns(tiles, (int)i, b.g, threads_ / 4, stage_grid_max_)))
                 append_stage_tiles(tiles, (int)i, b.g, threads_ / 4, ls.stage_budget, 4.0 * (2 * 18 + 8) * sizeof(R));
+            stage_len[i] = (int)(tiles.size() - t0);
             // this member's segment of the measurement list
             seg_off_[i] = (int)mtiles.size();
             append_measure_tiles(mtiles, (int)i, b.g, ls.meas_budget, 4.0 * 18 * sizeof(R));
@@ -339,7 +342,7 @@ public:
                              max_tiles_);
         const long long mt = (long long)mtiles.size();
         if (mt > mtiles_cap_) {
-            if (step_exec_ || meas_exec_) return set_error(ctx_, LGF_EINVAL, "measurement list grew after capture");
+            if (captured()) return set_error(ctx_, LGF_EINVAL, "measurement list grew after capture");
             LGF_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
             cudaFree(d_mtiles_);
             cudaFree(d_all_mtiles_);
@@ -351,7 +354,7 @@ public:
         long long rt = 0;
         for (auto* b : members) rt += b->g.n[0];
         if (rt > rtiles_cap_ || (long long)members.size() > jobs_cap_) {
-            if (step_exec_ || meas_exec_) return set_error(ctx_, LGF_EINVAL, "reduction list grew after capture");
+            if (captured()) return set_error(ctx_, LGF_EINVAL, "reduction list grew after capture");
             LGF_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
             cudaFree(d_rtiles_);
             cudaFree(d_jobs_);
@@ -361,16 +364,20 @@ public:
             LGF_CUDA_TRY(ctx_, cudaMalloc(&d_jobs_, sizeof(int) * jobs_cap_));
         }
         ntiles_ = (int)tiles.size();
-        // one page-locked area carries the descriptors, both tile lists and the count
+        // the stage's launch segments (unused slots empty)
+        std::vector<int2> segs = member_runs(stage_len, slots_, 8LL * stage_grid_max_);
+        stage_nseg_ = (int)segs.size();
+        segs.resize(slots_, make_int2(0, 0));
+        // one page-locked area carries the descriptors, both tile lists and the segments
         const size_t bd = align16(sizeof(LatDesc<R>) * members.size()), bt = align16(sizeof(int2) * tiles.size()),
-                     bm = align16(sizeof(int4) * mtiles.size());
+                     bm = align16(sizeof(int4) * mtiles.size()), bs = sizeof(int2) * slots_;
         std::lock_guard<std::mutex> lk(ctx_->list_mu);
         char* h = nullptr;
-        LGF_CUDA_TRY(ctx_, ctx_->list_stage.acquire(bd + bt + bm + 16, &h));
+        LGF_CUDA_TRY(ctx_, ctx_->list_stage.acquire(bd + bt + bm + bs, &h));
         std::memcpy(h, h_desc_.data(), sizeof(LatDesc<R>) * members.size());
         std::memcpy(h + bd, tiles.data(), sizeof(int2) * tiles.size());
         std::memcpy(h + bd + bt, mtiles.data(), sizeof(int4) * mtiles.size());
-        std::memcpy(h + bd + bt + bm, &ntiles_, sizeof(int));
+        std::memcpy(h + bd + bt + bm, segs.data(), bs);
         if (!members.empty())
             LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_desc_, h, sizeof(LatDesc<R>) * members.size(), cudaMemcpyHostToDevice,
                                                ctx_->stream));
@@ -380,7 +387,7 @@ public:
         if (mt)
             LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_all_mtiles_, h + bd + bt, sizeof(int4) * mtiles.size(),
                                                cudaMemcpyHostToDevice, ctx_->stream));
-        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_counts_, h + bd + bt + bm, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, cudaMemcpyAsync(d_seg_, h + bd + bt + bm, bs, cudaMemcpyHostToDevice, ctx_->stream));
         LGF_CUDA_TRY(ctx_, ctx_->list_stage.release(ctx_->stream));
         return LGF_OK;
     }
@@ -402,12 +409,14 @@ public:
     // assembled on the device (k_select_measure): no host wait.
     int set_measured(const std::vector<int>& which) override {
         if ((int)which.size() > max_members_) return set_error(ctx_, LGF_EINVAL, "measurement list exceeds capacity");
-        std::vector<int> sel(SEL_HEADER + SEL_FIELDS * which.size());
+        std::vector<int> sel(sel_ints((int)which.size()), 0);
+        std::vector<int> lens(which.size());
         long long tm = 0, tr = 0;
         for (size_t k = 0; k < which.size(); ++k) {
             const int i = which[k];
             if (i < 0 || i >= (int)members_.size()) return set_error(ctx_, LGF_EINVAL, "no member %d to measure", i);
-            int* f = &sel[SEL_HEADER + SEL_FIELDS * k];
+            lens[k] = seg_len_[i];
+            int* f = &sel[sel_fields() + SEL_FIELDS * k];
             f[0] = i;
             f[1] = seg_off_[i];
             f[2] = seg_len_[i];
@@ -422,6 +431,13 @@ public:
         sel[0] = (int)which.size();
         sel[1] = (int)tm;
         sel[2] = (int)tr;
+        // the measurement kernel's launch segments, over the selected members in list order
+        const std::vector<int2> segs = member_runs(lens, slots_, 8LL * meas_grid_max_);
+        for (size_t k = 0; k < segs.size(); ++k) {
+            sel[SEL_HEADER + 2 * k] = segs[k].x;
+            sel[SEL_HEADER + 2 * k + 1] = segs[k].y;
+        }
+        meas_nseg_ = (int)segs.size();
         {
             std::lock_guard<std::mutex> lk(ctx_->list_mu);
             char* h = nullptr;
@@ -431,90 +447,53 @@ public:
             LGF_CUDA_TRY(ctx_, ctx_->list_stage.release(ctx_->stream));
         }
         k_select_measure<<<dim3(std::max<int>(1, (int)which.size()), 16), 256, 0, ctx_->stream>>>(
-            d_sel_, d_all_mtiles_, d_mtiles_, d_rtiles_, d_jobs_, d_counts_ + 1);
+            d_sel_, sel_fields(), d_all_mtiles_, d_mtiles_, d_rtiles_, d_jobs_, d_counts_ + 1);
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
     }
 
-    int stage_grid() const { return dynamic_ ? stage_grid_max_ : std::max(1, std::min(ntiles_, stage_grid_max_)); }
-    int meas_grid() const {
-        return dynamic_ ? meas_grid_max_ : std::max(1, std::min((int)std::max<long long>(mtiles_cap_, 1), meas_grid_max_));
-    }
-
-    int launch_step() override {
-        if (!dynamic_ && ntiles_ == 0) return LGF_OK;
-        const int grid = stage_grid();
-        {
-            NvtxRange r("lgf.rk3_stage1");
-            k_rk3_stage<R, 1><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-        }
-        {
-            NvtxRange r("lgf.rk3_stage2");
-            k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-        }
-        {
-            NvtxRange r("lgf.rk3_stage3");
-            k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-        }
-        LGF_CUDA_TRY(ctx_, cudaGetLastError());
-        return LGF_OK;
-    }
+    int launch_step() override { return launch_stages(stage_nseg_); }
 
     // a single kernel: k = 0..2 stage k+1, k = 3 the measurement kernel alone
+    // (every launch segment of it)
     int launch_one(int k) override {
         if (k < 3) {
-            const int grid = stage_grid();
-            if (k == 0) k_rk3_stage<R, 1><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-            if (k == 1) k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
-            if (k == 2) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, d_counts_);
+            for (int j = 0; j < stage_nseg_; ++j) launch_stage(k + 1, j);
         } else {
-            launch_measure_kernel(meas_grid());
+            launch_measure_kernel(meas_nseg_);
         }
         LGF_CUDA_TRY(ctx_, cudaGetLastError());
         return LGF_OK;
     }
 
-    int launch_measure() override {
-        NvtxRange r("lgf.measure_launch");
-        const int mg = meas_grid();
-        const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
-        const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
-        launch_measure_kernel(mg);
-        k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
-        k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
-        LGF_CUDA_TRY(ctx_, cudaGetLastError());
-        return LGF_OK;
-    }
+    int launch_measure() override { return launch_measurement(meas_nseg_); }
 
+    // drop the graphs and capture those of the current segment counts
     int capture() override {
-        if (step_exec_) {
-            cudaGraphExecDestroy(step_exec_);
-            step_exec_ = nullptr;
-        }
-        if (meas_exec_) {
-            cudaGraphExecDestroy(meas_exec_);
-            meas_exec_ = nullptr;
-        }
-        int rc = capture_one(true, &step_exec_);
+        drop_graphs();
+        int rc = capture_one(true, stage_nseg_, &step_execs_[stage_nseg_]);
         if (rc != LGF_OK) return rc;
-        return capture_one(false, &meas_exec_);
+        return capture_one(false, meas_nseg_, &meas_execs_[meas_nseg_]);
     }
+    // graph launch; a graph per count of launch segments, captured on first use
     int replay_step() override {
         NvtxRange r("lgf.rk3_step");
-        if (!step_exec_) {
-            int rc = capture();
+        cudaGraphExec_t& g = step_execs_[stage_nseg_];
+        if (!g) {
+            int rc = capture_one(true, stage_nseg_, &g);
             if (rc != LGF_OK) return rc;
         }
-        LGF_CUDA_TRY(ctx_, cudaGraphLaunch(step_exec_, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, cudaGraphLaunch(g, ctx_->stream));
         return LGF_OK;
     }
     int replay_measure() override {
         NvtxRange r("lgf.measure");
-        if (!meas_exec_) {
-            int rc = capture();
+        cudaGraphExec_t& g = meas_execs_[meas_nseg_];
+        if (!g) {
+            int rc = capture_one(false, meas_nseg_, &g);
             if (rc != LGF_OK) return rc;
         }
-        LGF_CUDA_TRY(ctx_, cudaGraphLaunch(meas_exec_, ctx_->stream));
+        LGF_CUDA_TRY(ctx_, cudaGraphLaunch(g, ctx_->stream));
         return LGF_OK;
     }
     int launches_per_step() const override { return 3; }
@@ -522,19 +501,69 @@ public:
     const TileShape& shape() const override { return shape_; }
 
 private:
-    void launch_measure_kernel(int grid) {
-        if (shape_.meas_split == 2)
-            k_measure<R, false, 2><<<grid, dim3(MEAS_SITES, 12), measure_smem_bytes<R>(), ctx_->stream>>>(
-                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
-        else
-            k_measure<R, false, 1><<<grid, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
-                d_desc_, d_mtiles_, d_counts_ + 1, MeasOut{});
+    int stage_grid() const { return dynamic_ ? stage_grid_max_ : std::max(1, std::min(ntiles_, stage_grid_max_)); }
+    int meas_grid() const {
+        return dynamic_ ? meas_grid_max_ : std::max(1, std::min((int)std::max<long long>(mtiles_cap_, 1), meas_grid_max_));
+    }
+    // ints of a selection table for n members: header, launch segments, member fields
+    int sel_fields() const { return SEL_HEADER + 2 * slots_; }
+    size_t sel_ints(int n) const { return (size_t)sel_fields() + (size_t)SEL_FIELDS * std::max(n, 1); }
+    bool captured() const {
+        for (auto g : step_execs_) if (g) return true;
+        for (auto g : meas_execs_) if (g) return true;
+        return false;
+    }
+    void drop_graphs() {
+        for (auto& g : step_execs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        for (auto& g : meas_execs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     }
 
-    int capture_one(bool step, cudaGraphExec_t* out) {
+    // stage S over launch segment j of the tile list
+    void launch_stage(int S, int j) {
+        const int grid = stage_grid();
+        const int2* seg = d_seg_ + j;
+        if (S == 1) k_rk3_stage<R, 1><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, seg);
+        if (S == 2) k_rk3_stage<R, 2><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, seg);
+        if (S == 3) k_rk3_stage<R, 3><<<grid, threads_, 0, ctx_->stream>>>(d_desc_, d_tiles_, seg);
+    }
+    int launch_stages(int nseg) {
+        if (!dynamic_ && ntiles_ == 0) return LGF_OK;
+        static const char* names[3] = {"lgf.rk3_stage1", "lgf.rk3_stage2", "lgf.rk3_stage3"};
+        for (int S = 1; S <= 3; ++S) {
+            NvtxRange r(names[S - 1]);
+            for (int j = 0; j < nseg; ++j) launch_stage(S, j);
+        }
+        LGF_CUDA_TRY(ctx_, cudaGetLastError());
+        return LGF_OK;
+    }
+    int launch_measurement(int nseg) {
+        NvtxRange r("lgf.measure_launch");
+        const int rg = dynamic_ ? ctx_->sm_count : std::max(1, (int)std::min<long long>(rtiles_cap_, 4 * ctx_->sm_count));
+        const int jg = dynamic_ ? std::min(jobs_cap_, 4 * ctx_->sm_count) : std::max(1, (int)std::min<long long>(jobs_cap_, 4 * ctx_->sm_count));
+        launch_measure_kernel(nseg);
+        k_reduce_slices<R><<<rg, RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_rtiles_, d_counts_ + 2);
+        k_reduce_total<R><<<std::max(1, jg), RED_THREADS, 0, ctx_->stream>>>(d_desc_, d_jobs_, d_counts_ + 3);
+        LGF_CUDA_TRY(ctx_, cudaGetLastError());
+        return LGF_OK;
+    }
+    // the measurement kernel over launch segments 0..nseg-1 (read from the selection table)
+    void launch_measure_kernel(int nseg) {
+        const int grid = meas_grid();
+        const int2* segs = reinterpret_cast<const int2*>(d_sel_ + SEL_HEADER);
+        for (int j = 0; j < nseg; ++j) {
+            if (shape_.meas_split == 2)
+                k_measure<R, false, 2><<<grid, dim3(MEAS_SITES, 12), measure_smem_bytes<R>(), ctx_->stream>>>(
+                    d_desc_, d_mtiles_, segs + j, MeasOut{});
+            else
+                k_measure<R, false, 1><<<grid, dim3(MEAS_SITES, 6), measure_smem_bytes<R>(), ctx_->stream>>>(
+                    d_desc_, d_mtiles_, segs + j, MeasOut{});
+        }
+    }
+
+    int capture_one(bool step, int nseg, cudaGraphExec_t* out) {
         cudaGraph_t graph = nullptr;
         LGF_CUDA_TRY(ctx_, cudaStreamBeginCapture(ctx_->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = step ? launch_step() : launch_measure();
+        int rc = step ? launch_stages(nseg) : launch_measurement(nseg);
         cudaError_t e = cudaStreamEndCapture(ctx_->stream, &graph);
         if (rc != LGF_OK) {
             if (graph) cudaGraphDestroy(graph);
@@ -576,16 +605,19 @@ private:
     int* d_sel_ = nullptr;          // selection table of the next measurement
     int2* d_rtiles_ = nullptr;
     int* d_jobs_ = nullptr;
-    int* d_counts_ = nullptr;  // ntiles, nmtiles, nrtiles, njobs
+    int* d_counts_ = nullptr;  // (unused), nmtiles, nrtiles, njobs
     long long mtiles_cap_ = 0, rtiles_cap_ = 0;
     int jobs_cap_ = 0;
     int ntiles_ = 0;
     int stage_grid_max_ = 1, meas_grid_max_ = 1;
-    cudaGraphExec_t step_exec_ = nullptr, meas_exec_ = nullptr;
+    int slots_;                                   // launch slots per kernel (member_runs)
+    int stage_nseg_ = 1, meas_nseg_ = 1;           // launch segments in use
+    int2* d_seg_ = nullptr;                        // the stage's launch segments
+    std::vector<cudaGraphExec_t> step_execs_, meas_execs_;  // by segment count
 };
 
 GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
-                      bool dynamic, bool per_volume) {
+                      bool dynamic, bool per_volume, int launch_slots) {
     if (shape.threads < 128 || shape.threads % 128 || shape.threads > stage_max_threads(precision) ||
         (shape.meas_split != 1 && shape.meas_split != 2) || shape.stage_budget <= 0 || shape.meas_budget <= 0) {
         set_error(ctx, LGF_EINVAL, "invalid tile shape (threads %d, measurement split %d)", shape.threads,
@@ -594,11 +626,11 @@ GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int m
     }
     GroupBase* g = nullptr;
     if (precision == LGF_PREC_FP64) {
-        auto* p = new (std::nothrow) Group<double>(ctx, shape, max_members, max_tiles, dynamic, per_volume);
+        auto* p = new (std::nothrow) Group<double>(ctx, shape, max_members, max_tiles, dynamic, per_volume, launch_slots);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     } else {
-        auto* p = new (std::nothrow) Group<float>(ctx, shape, max_members, max_tiles, dynamic, per_volume);
+        auto* p = new (std::nothrow) Group<float>(ctx, shape, max_members, max_tiles, dynamic, per_volume, launch_slots);
         if (p && p->init() != LGF_OK) { delete p; p = nullptr; }
         g = p;
     }
@@ -792,14 +824,15 @@ template <typename R> static int single_lattice_measure(lgf_ctx* ctx, LatticeBuf
     d.nchunk = b.nchunk;
     void* ddesc = nullptr;
     int4* dmt = nullptr;
-    int* dn = nullptr;
+    int2* dn = nullptr;
+    const int2 seg = make_int2(0, n);
     cudaError_t e = prepare_measure_kernel<R, true>();
     if (e == cudaSuccess) e = cudaMalloc(&ddesc, sizeof d);
     if (e == cudaSuccess) e = cudaMalloc(&dmt, sizeof(int4) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dn, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&dn, sizeof(int2));
     if (e == cudaSuccess) e = cudaMemcpyAsync(ddesc, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dmt, mt.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &seg, sizeof(int2), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         k_measure<R, true><<<std::min(n, 4 * ctx->sm_count), dim3(MEAS_SITES, MEAS_WARPS), measure_smem_bytes<R, true>(),
                              ctx->stream>>>((const LatDesc<R>*)ddesc, dmt, dn, out);

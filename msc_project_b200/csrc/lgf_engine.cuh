@@ -185,9 +185,11 @@ public:
 };
 
 // dynamic: members change after the graphs are captured; per_volume: each
-// member's lists follow the work order tuned for its own volume class
+// member's lists follow the work order tuned for its own volume class;
+// launch_slots: each kernel runs as up to this many launches, one per run of
+// whole members (member_runs: large lattices get launches of their own)
 GroupBase* make_group(lgf_ctx* ctx, int precision, const TileShape& shape, int max_members, long long max_tiles,
-                      bool dynamic, bool per_volume = false);
+                      bool dynamic, bool per_volume = false, int launch_slots = 1);
 
 int launch_reunitarize(lgf_ctx* ctx, LatticeBuf& b);
 int launch_to_device(lgf_ctx* ctx, LatticeBuf& b, const double* dev_file_order);

@@ -146,7 +146,8 @@ template <typename R> struct LatDesc {
 //   S=3:                             U3 = exp(eps (3/4 Z2 - A)) U2
 // which equals GradientFlow.cpp:27-50 term by term.  Input and output are
 // different buffers of the ring (every thread reads neighbours of the input).
-// Persistent: blocks stride over the tile list; tile = (lattice, first site).
+// Persistent: blocks stride over one segment of the tile list (seg = first
+// tile, count); tile = (lattice, first site).
 // A tile of T threads (T a multiple of 128) covers T/4 consecutive sites with
 // all four directions: warp w handles mu = w % 4 for the 32 sites of group
 // w / 4, so the four link directions of a site range are read together and
@@ -156,9 +157,9 @@ template <> struct StageMaxThreads<double> { static constexpr int value = LGF_ST
 
 template <typename R, int S>
 __global__ void __launch_bounds__(StageMaxThreads<R>::value, LGF_STAGE_MINB) k_rk3_stage(const LatDesc<R>* __restrict__ descs, const int2* __restrict__ tiles,
-                                                   const int* __restrict__ ntiles) {
-    const int n = *ntiles;
-    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+                                                   const int2* __restrict__ seg) {
+    const int2 r = *seg;  // this launch's tiles: tiles[r.x, r.x + r.y)
+    for (int ti = r.x + blockIdx.x; ti < r.x + r.y; ti += gridDim.x) {
         const int2 tile = tiles[ti];
         const LatDesc<R>* d = descs + tile.x;
         const Geom g = d->g;
@@ -666,15 +667,15 @@ __device__ __forceinline__ void plane_fields_smem(const cplx<R>* __restrict__ U,
 template <typename R, bool OUT = false, int QS = MEAS_QSPLIT>
 __global__ void __launch_bounds__(MEAS_SITES * 6 * QS, MeasMinBlocks<QS>::value) k_measure(const LatDesc<R>* __restrict__ descs,
                                                                            const int4* __restrict__ mtiles,
-                                                                           const int* __restrict__ nmtiles,
+                                                                           const int2* __restrict__ seg,
                                                                            MeasOut out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MeasSmem<R, OUT>* sm = reinterpret_cast<MeasSmem<R, OUT>*>(smem_raw);
     const int lane = threadIdx.x, w = threadIdx.y, p = w % 6, part = w / 6;
     constexpr int NW = 6 * QS;  // warps of the block
     const int qa = part * 2, qb = qa + 2;  // QS = 2: this warp's quadrant half
-    const int n = *nmtiles;
-    for (int ti = blockIdx.x; ti < n; ti += gridDim.x) {
+    const int2 r = *seg;  // this launch's tiles: mtiles[r.x, r.x + r.y)
+    for (int ti = r.x + blockIdx.x; ti < r.x + r.y; ti += gridDim.x) {
         const int4 tile = mtiles[ti];
         const LatDesc<R>* d = descs + tile.x;
         const Geom g = d->g;

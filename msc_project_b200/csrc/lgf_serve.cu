@@ -329,7 +329,8 @@ int lgf_server::tick(std::vector<ServeJob*>& act) {
     for (int p = 0; p < 2; ++p) {
         if (byprec[p].empty()) continue;
         if (!group[p]) {
-            group[p].reset(make_group(ctx, p, shape[p], std::max(cfg.max_active, 1), max_tiles[p], true, true));
+            group[p].reset(make_group(ctx, p, shape[p], std::max(cfg.max_active, 1), max_tiles[p], true, true,
+                                          std::min(std::max(cfg.max_active, 1), 32)));
             if (!group[p]) return LGF_ENOMEM;
         }
         std::vector<LatticeBuf*> m;
