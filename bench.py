@@ -371,12 +371,15 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
     from msc_project_b200 import FP32MIXED, Job, Server
     rng = np.random.default_rng(seed)
     vols = [(16, 16, 16, 16), (48, 24, 24, 24), (32, 32, 32, 32), (48, 48, 48, 48)]
-    jobs = []
+    specs = []
     for i in range(njobs):
         shape = vols[int(rng.integers(0, 4))]
         tmax = float(rng.uniform(1.0, 8.0))
-        jobs.append(Job(shape, FP32MIXED, seed=1000 + i, nsteps=int(round(tmax / 0.01)), meas_every=5,
-                        reunit_every=10))
+        specs.append((shape, 1000 + i, int(round(tmax / 0.01))))
+
+    def make_jobs():
+        return [Job(shape, FP32MIXED, seed=sd, nsteps=n, meas_every=5, reunit_every=10) for shape, sd, n in specs]
+    jobs = make_jobs()
     # rate = inf: every job arrives at t = 0 (the saturated server)
     gaps = np.zeros(njobs) if not np.isfinite(rate) else rng.exponential(1.0 / rate, size=njobs)
     try:
@@ -399,11 +402,18 @@ def form_served(ctx, njobs: int, rate: float, seed: int = 5):
         stats = srv.stats()
     lat = np.array([s.end_s - s.submit_s for s in sts])
     work = sum(int(np.prod(j.shape)) * j.nsteps for j in jobs)
-    return {"jobs": njobs, "rate_per_s": rate if np.isfinite(rate) else "all at t=0", "jobs_per_s": njobs / makespan,
-            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-            "site_steps_per_s": work / makespan, "hbm_budget_bytes": budget,
-            "device_busy_frac": stats["device_busy_s"] / stats["wall_s"], "server_stats": stats,
-            "all_done": all(s.state == 2 for s in sts)}
+    out = {"jobs": njobs, "rate_per_s": rate if np.isfinite(rate) else "all at t=0", "jobs_per_s": njobs / makespan,
+           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+           "site_steps_per_s": work / makespan, "hbm_budget_bytes": budget,
+           "device_busy_frac": stats["device_busy_s"] / stats["wall_s"], "server_stats": stats,
+           "all_done": all(s.state == 2 for s in sts)}
+    if not np.isfinite(rate):
+        # the same jobs as one offline batch (lgf_batch_run): what continuous
+        # batching costs against knowing every job up front
+        st = ctx.batch_run(make_jobs())
+        out["batched_same_jobs_site_steps_per_s"] = st.site_steps / st.seconds
+        out["vs_batched_same_jobs"] = out["site_steps_per_s"] / out["batched_same_jobs_site_steps_per_s"]
+    return out
 
 
 def form_heatbath(ctx):
