@@ -431,7 +431,7 @@ template <int QS> struct MeasMinBlocks { static constexpr int value = QS == 2 ? 
 // quadrant of the site reuses them), then the per-plane results.
 template <typename R, bool OUT> struct MeasSmem {
     union {
-        R line[8][2][18][MEAS_SITES];  // [2*dir + (sign<0)][length-2][entry][site]
+        R line[8][2][2 * MEAS_STASH_ENTRIES][MEAS_SITES];  // [2*dir + (sign<0)][length-2][real of entry][site]
         struct {                       // after the lines are dead: the second quadrant half's sums
             alg<R> G[6][MEAS_SITES];
             alg<R> Fh[6][MEAS_SITES];
@@ -458,10 +458,12 @@ struct MeasOut {
     double2* dbg_improved;
 };
 
+// A line is only ever extended (the left operand of a product that rebuilds
+// the third row), so like a parked path it keeps its first two rows.
 template <typename R, bool OUT>
 __device__ __forceinline__ void store_line(MeasSmem<R, OUT>* sm, int sdir, int len, int lane, const su3<R>& L) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
+    for (int k = 0; k < MEAS_STASH_ENTRIES; ++k) {
         sm->line[sdir][len - 2][2 * k][lane] = L.m[k].re;
         sm->line[sdir][len - 2][2 * k + 1][lane] = L.m[k].im;
     }
@@ -470,7 +472,10 @@ template <typename R, bool OUT>
 __device__ __forceinline__ su3<R> load_line(const MeasSmem<R, OUT>* sm, int sdir, int len, int lane) {
     su3<R> L;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) L.m[k] = cmk<R>(sm->line[sdir][len - 2][2 * k][lane], sm->line[sdir][len - 2][2 * k + 1][lane]);
+    for (int k = 0; k < 9; ++k)
+        L.m[k] = k < MEAS_STASH_ENTRIES
+                     ? cmk<R>(sm->line[sdir][len - 2][2 * k][lane], sm->line[sdir][len - 2][2 * k + 1][lane])
+                     : cmk<R>(R(0), R(0));  // never read: the next product rebuilds the row
     return L;
 }
 

@@ -108,7 +108,11 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
             t.stage_budget = mb * MB;
             try_stage(t);
         }
-    // ---- measurement kernel alone
+    // ---- measurement kernel alone, starting from whole-slice blocks (the
+    // fewest DRAM bytes: 1.59x the link bytes against 2.05x for 2 MB blocks
+    // on 24^3x48); smaller blocks replace them only when 2% faster (on 48^4
+    // whole slices no longer fit L2 and are 45% slower)
+    cur.meas_budget = 64.0 * MB;
     float meas_ms = 0.f;
     if (rc == LGF_OK) rc = time_shape(ctx, prec, b, cur, 3, 1, &probe);
     const int mreps = std::max(3, std::min(200, (int)(TARGET_MS / std::max(probe, 1e-3f))));
@@ -127,7 +131,7 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
         t.meas_split = 3 - cur.meas_split;
         try_meas(t);
     }
-    for (double mb : {2.0, 8.0, 64.0}) {
+    for (double mb : {8.0, 2.0}) {
         TileShape t = cur;
         t.meas_budget = mb * MB;
         try_meas(t);

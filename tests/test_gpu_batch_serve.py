@@ -74,6 +74,27 @@ def test_server_alone_vs_mix_and_latency(ctx):
     assert np.percentile(lat, 99) >= np.percentile(lat, 50) > 0
 
 
+def test_server_launch_segments_alone_vs_mix(ctx):
+    """Resident jobs large enough for launch segments of their own (each
+    kernel launched once per job, small jobs sharing one) give the same bits
+    as each job flowed alone."""
+    def jobs():
+        return [Job((16, 16, 24, 24), FP64, seed=201, nsteps=6, meas_every=2, want_links=True),
+                Job((8, 8, 8, 8), FP64, seed=202, nsteps=6, meas_every=3, want_links=True),
+                Job((4, 4, 6, 6), FP64, seed=205, nsteps=5, meas_every=1, want_links=True),
+                Job((16, 16, 24, 24), FP64, seed=203, nsteps=4, meas_every=2, want_links=True),
+                Job((24, 16, 16, 16), FP32MIXED, seed=204, nsteps=6, meas_every=2, reunit_every=3, want_links=True)]
+    refs = [alone(ctx, j) for j in jobs()]
+    mix = jobs()
+    with Server(ctx, 1 << 33, max_active=5, steps_per_tick=2) as srv:
+        ids = [srv.submit(j) for j in mix]
+        sts = [srv.wait(i, 120.0) for i in ids]
+    for j, st, (r, links) in zip(mix, sts, refs):
+        assert st.state == C.LGF_JOB_DONE and st.error == 0
+        assert np.array_equal(j.result.E, r.E) and np.array_equal(j.result.Q, r.Q)
+        assert np.array_equal(j.links_out, links)
+
+
 def test_server_rejects_jobs_that_never_fit(ctx):
     with Server(ctx, 1 << 20, max_active=2) as srv:
         with pytest.raises(LGFError) as e:
