@@ -233,7 +233,7 @@ typedef struct lgf_server lgf_server;
 
 typedef struct lgf_serve_config {
     size_t hbm_budget_bytes;   /* admission budget for resident jobs (links + RK3 scratch) */
-    int max_active;            /* maximum concurrently flowing jobs (slots) */
+    int max_active;            /* maximum concurrently flowing jobs (slots; up to 32 of them get launches of their own) */
     int steps_per_tick;        /* RK3 steps per scheduling tick */
 } lgf_serve_config;
 
