@@ -541,22 +541,13 @@ void lgf_server::run() {
     if (snap_thread.joinable()) snap_thread.join();
 }
 
-// Tile shape for the shared launches of one precision: the tuned shape of the
-// context's tuned volume nearest to 2^20 sites (the middle of the served
-// volumes), else the default.
-static TileShape serve_shape(const lgf_ctx* ctx, int prec) {
-    TileShape best = default_shape(prec);
-    double dist = 1e300;
-    for (const auto& t : ctx->tuned) {
-        if (t.prec != prec) continue;
-        const double d = std::fabs(std::log((double)t.volume / (double)(1 << 20)));
-        if (d < dist) {
-            dist = d;
-            best = t.shape;
-        }
-    }
-    return best;
-}
+// Kernel shape (block size, measurement warps per plane) of the shared
+// launches of one precision: the defaults.  A shape tuned on one volume
+// class is not carried over to every job of a mix: a one-warp-per-plane
+// measurement tuned (by under 2%) on 24^3x48 slowed a served mix of four
+// volumes by 12%.  Each job's work order is still its own class's tuned
+// order (the groups' per-volume lists).
+static TileShape serve_shape(const lgf_ctx*, int prec) { return default_shape(prec); }
 
 extern "C" {
 
