@@ -3,7 +3,7 @@
 Runs oracle/_ref/lgf_ref (the unmodified reference sources compiled by
 oracle/Makefile with the single-rank MPI stub and the seed shim) and writes:
 
-  hb8_seed1.bin            config 1 input: reference heatbath, beta=6.0, seed 1,
+  hb8_seed1.bin            8^4 input: reference heatbath, beta=6.0, seed 1,
                            8^4, 200 x (Cabibbo-Marinari + 5 OR) sweeps, saved
                            configuration #0 (reference file layout, 2.36 MB)
   flow8_hb_seed1.json      FlowSavedGaugeConfigurations on it: eps=0.01, 100
@@ -117,7 +117,7 @@ def reference_resume(work: Path, out: Path):
 def reference_measure_workflows(tmp: Path, out_json: Path, out_q: Path):
     """The reference's MeasureQdensityDistribution and
     MeasureFlowedGaugeConfigurations (LGF/LGF.cpp:113-123, :228-255) on the
-    config-1 flow's saved t = 1.0 links (FlowParameters(0, 0, 100, 0.01, 1)),
+    8^4 heatbath flow's saved t = 1.0 links (FlowParameters(0, 0, 100, 0.01, 1)),
     each in a fresh folder holding only that file."""
     shape = (8, 8, 8, 8)
     rel = Path("ensembles") / "su3" / BETA_DIR / shape_dir(shape) / "GF"
@@ -218,7 +218,7 @@ def main():
         return
     with tempfile.TemporaryDirectory() as tmp:
         tmp = Path(tmp)
-        # ---- config 1: heatbath input + 8^4 flow
+        # ---- 8^4 heatbath input + its flow
         hb = HERE / "hb8_seed1.bin"
         if not args.skip_heatbath or not hb.exists():
             run_ref(["heatbath", str(tmp / "hb") + "/", "6.0", 8, 8, 8, 8, 200, 5], env={"LGF_REF_SEED": "1"})

@@ -11,14 +11,14 @@ pytestmark = pytest.mark.gpu
 CLI = ROOT / "msc_project_b200" / "lgf_flow"
 
 
-def place_config1(tmp_path):
+def place_hb8_input(tmp_path):
     d = tmp_path / "ensembles/su3/beta6_000000/8X8X8X8/LHMC_3_of_0_330000"
     d.mkdir(parents=True)
     (d / "torus_extdof4_0.bin").write_bytes((GOLDEN / "hb8_seed1.bin").read_bytes())
 
 
 def test_cli_flow_matches_reference_csv(tmp_path):
-    place_config1(tmp_path)
+    place_hb8_input(tmp_path)
     g = golden_json("flow8_hb_seed1.json")
     r = subprocess.run([str(CLI), "4", "4", "6.0", "8", "8", "8", "8", "0", "0", "0", "0", "0", "0", "100", "0.01",
                         "1", str(tmp_path) + "/"], capture_output=True, text=True, timeout=300)
@@ -33,7 +33,7 @@ def test_cli_flow_matches_reference_csv(tmp_path):
 
 
 def test_cli_fp32mixed(tmp_path):
-    place_config1(tmp_path)
+    place_hb8_input(tmp_path)
     r = subprocess.run([str(CLI), "4", "4", "6.0", "8", "8", "8", "8", "0", "0", "0", "0", "0", "0", "100", "0.01",
                         "10", str(tmp_path) + "/", "--precision", "fp32mixed"], capture_output=True, text=True,
                        timeout=300)

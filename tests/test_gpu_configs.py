@@ -81,7 +81,7 @@ def test_dropin_16_4_t3_csv_bytes_match_reference(ctx, tmp_path):
                          np.array(g["flowed_sites"]))) < TOL
 
 
-def test_config3_fp32mixed_gates_32_4_t5(ctx):
+def test_fp32mixed_gates_32_4_t5(ctx):
     shape, steps, meas = (32, 32, 32, 32), 500, 10
     res = {}
     for prec, reunit in ((FP64, 0), (FP32MIXED, 10)):
@@ -103,7 +103,7 @@ ENSEMBLE = [((8, 8, 8, 8), 16), ((12, 12, 12, 12), 16), ((16, 16, 16, 16), 16), 
             ((48, 24, 24, 24), 8)]
 
 
-def test_config4_ensemble_fp32mixed_gates(ctx):
+def test_ensemble_of_64_fp32mixed_gates(ctx):
     runs = {}
     for prec, reunit in ((FP64, 0), (FP32MIXED, 10)):
         jobs, seed = [], 100

@@ -1,7 +1,7 @@
 """GPU configuration generation: hot/cold start, Cabibbo-Marinari heatbath and
 overrelaxation.  The reference seeds from std::random_device, so the heatbath
 is compared statistically with the reference's own heatbath configuration (the
-config-1 input, beta = 6.0, 200 x (CM + 5 OR)); overrelaxation has an exact
+8^4 input, beta = 6.0, 200 x (CM + 5 OR)); overrelaxation has an exact
 invariant (the Wilson action)."""
 import numpy as np
 import pytest

@@ -360,7 +360,7 @@ def test_unaligned_volume_against_oracle(ctx):
 
 def test_resume_against_reference(ctx, tmp_path):
     """The reference's own ResumeFlowedConfiguration (LGF.cpp:197-226) run on
-    its config-1 flow: pick up t = 1.0, 50 steps measuring every 5.  The
+    its 8^4 heatbath flow: pick up t = 1.0, 50 steps measuring every 5.  The
     drop-in's appended CSV files are byte-identical, E(t)/Q(t) agree to 1e-12
     and the saved t = 1.5 links to 1e-11."""
     from msc_project_b200 import (FlowParameters, FlowSavedGaugeConfigurations, ResumeFlowedConfiguration,
@@ -391,7 +391,7 @@ def test_resume_against_reference(ctx, tmp_path):
 
 def test_measure_workflows_against_reference(ctx, tmp_path):
     """The reference's own MeasureFlowedGaugeConfigurations and
-    MeasureQdensityDistribution (LGF.cpp:228-255, :113-123) on its config-1
+    MeasureQdensityDistribution (LGF.cpp:228-255, :113-123) on its 8^4 heatbath
     t = 1.0 links: improved E and clover Q to 1e-12 with byte-identical CSV
     files, and the q-density file (with its pi^2/4 prefactor) to 1e-12."""
     from msc_project_b200 import (FlowParameters, FlowSavedGaugeConfigurations, MeasureFlowedGaugeConfigurations,
@@ -445,7 +445,7 @@ def test_flow_four_extents_against_reference(ctx, prec):
 
 
 def test_long_flow_against_oracle(ctx):
-    """500 RK3 steps (t = 5) of the config-1 input: the flow is contracting,
+    """500 RK3 steps (t = 5) of the 8^4 heatbath input: the flow is contracting,
     so the GPU and the oracle stay together to rounding over a long flow
     (E, Q every 100 steps and the final links)."""
     shape = (8, 8, 8, 8)
