@@ -109,7 +109,7 @@ int tune_shape(lgf_ctx* ctx, int prec, const int shape[4], TileShape* best) {
             try_stage(t);
         }
     // ---- measurement kernel alone, starting from whole-slice blocks (the
-    // fewest DRAM bytes: 1.59x the link bytes against 2.05x for 2 MB blocks
+    // fewest DRAM bytes: 1.16x the link bytes against 2.05x for 2 MB blocks
     // on 24^3x48); smaller blocks replace them only when 2% faster (on 48^4
     // whole slices no longer fit L2 and are 45% slower)
     cur.meas_budget = 64.0 * MB;
